@@ -1,0 +1,185 @@
+/*
+ * udock_b200.h -- C ABI of the B200 docking engine (libudock_b200.so).
+ *
+ * The engine replaces the hot path behind the reference's pybind module
+ * `unidock_engine.api.python.pipeline` (reference: unidock/unidock_engine/api/python/
+ * pipeline.cpp:56-151).  The reference binds C++ classes; this library exports plain
+ * C functions over pointers and sizes so any FFI (ctypes, cffi, JNI, cgo) can bind it.
+ * Each function below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns 0 on success and a negative code on failure; the message
+ *    of the last failure on the calling thread is returned by ud_last_error()
+ *    (reference: exceptions -> core_pipeline() returns 1 -> RuntimeError,
+ *    src/screening/core.cpp:218-222, api/python/pipeline.cpp:141-143).
+ *  - All arrays are caller-owned host memory, C-contiguous; the engine copies what it
+ *    keeps.  Device memory is owned by the context and freed by ud_destroy.
+ *  - Calls on one context are synchronous and not re-entrant; different contexts may
+ *    be used from different threads.
+ *  - Angles are radians; coordinates Angstrom; energies kcal/mol.
+ *  - A pose record is [energy, cx, cy, cz, rvx, rvy, rvz, 0, coords(3N), dihedrals(T)]:
+ *    the reference's FlexPose (src/model/model.h:18-24) flattened.
+ */
+#ifndef UDOCK_B200_H
+#define UDOCK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ud_ctx ud_ctx;
+
+enum { UD_OK = 0, UD_EINVAL = -1, UD_ECUDA = -2, UD_ESTATE = -3, UD_ENOMEM = -4 };
+enum { UD_MODE_DIRECT = 0, UD_MODE_GRID = 1 };
+enum { UD_GRID_F32 = 0, UD_GRID_F16 = 1 };
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ud_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ud_last_error(void);
+
+/* Create a context on CUDA device `device` for the docking box
+ * box6 = {x_lo, x_hi, y_lo, y_hi, z_lo, z_hi}.
+ * Replaces: DockingPipeline(...) construction + decide_memory_limit_mb/cudaSetDevice
+ * (api/python/pipeline.cpp:58-111, src/screening/core.cpp:32-63). */
+int ud_create(int device, const float* box6, ud_ctx** out);
+
+/* Free all device memory of the context (src/task/DockTask.cpp free_memory_all). */
+int ud_destroy(ud_ctx* ctx);
+
+/* Search flags: constraint docking (no translation/rotation), bias type
+ * (0 none, 1 position, 2 z-align) and bias scale.
+ * Replaces: apply_bias / constraint_docking handling (src/screening/core.cpp:86-97,142-146). */
+int ud_set_flags(ud_ctx* ctx, int constraint_docking, int bias_type, float bias_k);
+
+/* Receptor atoms; hydrogens and atoms outside the box grown by 8 A are dropped here.
+ * Replaces: DockingPipeline.set_receptor + RapidJsonParser::parse_receptor_info
+ * (api/python/pipeline.cpp:113-116, src/format/rapidjson_parser.cpp:25-52). */
+int ud_set_receptor(ud_ctx* ctx, int n, const float* xyz, const int* types);
+
+/* Number of receptor atoms kept. */
+int ud_receptor_count(const ud_ctx* ctx);
+
+/* Build per-type grid maps covering the box at `spacing` for the XS types in
+ * map_types[nmaps] (1..20 non-hydrogen types); precision selects the map storage used by searches
+ * (UD_GRID_F32, or UD_GRID_F16 kept beside the FP32 master).
+ * New component (the reference scores by direct pair sum, src/cuda/bfgs.cuh:242-289). */
+int ud_build_grid(ud_ctx* ctx, float spacing, int nmaps, const int* map_types, int precision);
+
+/* Copy the FP32 maps to the host (out: nmaps*gz*gy*gx floats, x fastest); gdim3 and
+ * origin3 receive the grid shape and origin.  Pass out=NULL to query the shape only. */
+int ud_get_grid(const ud_ctx* ctx, float* out, int* gdim3, float* origin3);
+
+/* Select the map storage used for grid-mode scoring (UD_GRID_F32 / UD_GRID_F16). */
+int ud_set_grid_precision(ud_ctx* ctx, int precision);
+
+/* Append ligands.  All index arrays are local to the ligand.  Offsets are prefix sums
+ * of length count+1 into the following array:
+ *   atom_off[nlig+1]   -> xyz (3 per atom), types
+ *   tors_off[nlig+1]   -> axis (2 per torsion: from,to), dihedrals (radians)
+ *   range_off[T+1]     -> ranges (2 per range, radians); T = tors_off[nlig]
+ *   rot_off[T+1]       -> rot_atoms (atoms moved by each torsion)
+ *   pair_off[A+1]      -> pairs (per-atom intra neighbours, both directions); A = atom_off[nlig]
+ *   bias_off[A+1]      -> bias (5 per record: x y z V r2); bias_off/bias may be NULL
+ * Replaces: DockingPipeline.add_ligands + RapidJsonParser::parse_ligands_info and the
+ * GPU upload of DockTask::alloc_gpu (api/python/pipeline.cpp:118-123,
+ * src/format/rapidjson_parser.cpp:54-225, src/cuda/task.cu:304-402). */
+int ud_add_ligands(ud_ctx* ctx, int nlig, const int* atom_off, const float* xyz, const int* types,
+                   const int* tors_off, const int* axis, const float* dihedrals,
+                   const int* range_off, const float* ranges, const int* rot_off, const int* rot_atoms,
+                   const int* pair_off, const int* pairs, const int* bias_off, const float* bias);
+
+/* Drop all ligands and search results. */
+int ud_clear_ligands(ud_ctx* ctx);
+
+/* Number of ligands loaded. */
+int ud_ligand_count(const ud_ctx* ctx);
+
+/* Energy and generalised gradient (6+T: centre, orientation, torsions) of n poses.
+ * pose_lig[n] ligand index per pose; coords concatenated per pose (3*natom each);
+ * centers/rotvecs 3 per pose (rotvec = last rotation increment, the reference's
+ * FlexPose::rot_vec); out_g concatenated 6+T per pose.
+ * mode UD_MODE_DIRECT (reference pair sum) or UD_MODE_GRID.
+ * Replaces: cal_e_grad_one_gpu (src/cuda/bfgs_wrapper.cu:63-98), batched. */
+int ud_score_batch(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, const float* centers,
+                   const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g);
+
+/* Final-score terms of n poses without curl: out_terms4 = [intra(i<j), inter, penalty, bias]
+ * per pose; out_decomp (nullable) = 5 inter terms per atom
+ * [gauss1, gauss2, repulsion, hydrophobic, hbond].
+ * Replaces: score() / score_decomp() (src/score/score.cpp:12-147). */
+int ud_score_terms(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, int mode,
+                   float* out_terms4, float* out_decomp);
+
+/* In-place BFGS of n pose records (see header comment; records concatenated, record of a
+ * pose sized for its ligand).  `rounds` consecutive optimisations of max_steps each,
+ * round r using penalty slope min(slope0 * 100^r, 1e6) when ramp != 0, else slope0.
+ * out_nevals (nullable) receives energy evaluations per pose.
+ * Replaces: opt_kernel / optimize_cu and DockTask::run_refine
+ * (src/cuda/optimize.cu:14-77, src/task/DockTask.cpp:155-186). */
+int ud_bfgs_batch(ud_ctx* ctx, int n, const int* pose_lig, float* records, int max_steps, int rounds,
+                  float vcap, float slope0, int ramp, int mode, int* out_nevals);
+
+/* Monte Carlo search: nchain chains per loaded ligand, one persistent launch; each
+ * chain keeps its best pose.  opt_steps >= 0 (resolve the reference's -1 heuristic
+ * on the host).  out_nevals (nullable) receives the total energy evaluations.
+ * Replaces: mc_cu / mc_kernel / randomize_pose (src/cuda/mc.cu:18-448). */
+int ud_search(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
+              int mode, long long* out_nevals);
+
+/* Best pose record of every chain of ligand `lig` (nchain records, ligand-sized). */
+int ud_get_chain_poses(const ud_ctx* ctx, int lig, float* out_records);
+
+/* Size in floats of one pose record of ligand `lig`. */
+int ud_record_floats(const ud_ctx* ctx, int lig);
+
+/* Greedy RMSD clustering of each ligand's chain poses (heavy atoms, no fit; stable
+ * energy order, ties by index; a pose is kept iff its squared deviation sum to every
+ * kept pose is >= limit^2 * n_heavy).  out_leaders[nlig*nchain] (chain indices, sorted
+ * by energy), out_counts[nlig].
+ * Replaces: cluster_cu (src/cuda/cluster.cu:74-135). */
+int ud_cluster(ud_ctx* ctx, float rmsd_limit, int* out_leaders, int* out_counts);
+
+/* Full docking of all loaded ligands: search, clustering, refinement of the cluster
+ * leaders (refine_steps rounds x 2 BFGS steps, slope ramp 1e2..1e6, vcap 1000), filter
+ * by energy_range and num_pose, final scoring (no curl, direct sum).
+ * Replaces: DockTask::run (src/task/DockTask.cpp:39-123) over all batches. */
+typedef struct {
+    uint64_t seed;
+    int nchain;          /* exhaustiveness */
+    int mc_steps;
+    int opt_steps;       /* resolved, >= 0 */
+    int refine_steps;
+    int num_pose;
+    float rmsd_limit;
+    float energy_range;
+    int randomize;
+    int mode;            /* UD_MODE_GRID or UD_MODE_DIRECT for the search */
+    int final_mode;      /* scoring of output poses: UD_MODE_DIRECT (reference) or grid */
+    int energy_decomp;
+} ud_dock_params;
+
+int ud_dock(ud_ctx* ctx, const ud_dock_params* params, long long* out_nevals);
+
+/* Output pose counts per ligand after ud_dock (out_counts[nlig]). */
+int ud_result_counts(const ud_ctx* ctx, int* out_counts);
+
+/* Output poses after ud_dock, ligand-major, in rank order:
+ * out_records: pose records (ligand-sized, concatenated);
+ * out_terms4: [intra, inter, penalty, bias] per pose;
+ * out_decomp (nullable, only if energy_decomp): 5 per atom per pose. */
+int ud_get_results(const ud_ctx* ctx, float* out_records, float* out_terms4, float* out_decomp);
+
+/* Total floats of all output records (sizing helper for ud_get_results). */
+long long ud_result_floats(const ud_ctx* ctx);
+
+/* Synchronise the context's stream; returns an error if a kernel failed. */
+int ud_sync(ud_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,155 @@
+"""GPU parity for the optimiser, the MC search, clustering and the full docking path."""
+import numpy as np
+import pytest
+
+from gpu_helpers import engine_for, oracle_grid, perturbed_poses
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu_sys(small_system, oracle64):
+    eng, mt = engine_for(small_system)
+    ogrid, _ = oracle_grid(oracle64, small_system, eng)
+    return dict(eng=eng, mt=mt, ogrid=ogrid, **small_system)
+
+
+def _starts(gpu_sys, oracle, rng, per_lig):
+    from ud2b200 import make_record
+    env = oracle.make_env(gpu_sys["rec"], gpu_sys["box"], grid=gpu_sys["ogrid"], mode="grid")
+    pl, recs, poses = [], [], []
+    for li, lig in enumerate(gpu_sys["ligs"]):
+        olig = oracle.ligand(lig)
+        for p in perturbed_poses(oracle, olig, env, lig, rng, per_lig, gpu_sys["box"]):
+            pl.append(li)
+            poses.append(p)
+            recs.append(make_record(lig, p["coords"], p["center"], p["rot_vec"], p["dihedrals"]))
+    return env, pl, recs, poses
+
+
+def test_bfgs_same_minimum_as_oracle(gpu_sys, oracle64):
+    """BFGS from identical starts run to convergence reaches the oracle's minimum within
+    1e-3 kcal/mol (FP32 kinematics/scoring, FP64 inverse Hessian vs all-FP64 oracle)."""
+    from ud2b200 import MODE_GRID, split_record
+    eng = gpu_sys["eng"]
+    rng = np.random.default_rng(21)
+    env, pl, recs, poses = _starts(gpu_sys, oracle64, rng, 8)
+    out, ne = eng.bfgs_batch(pl, recs, max_steps=400, rounds=1, vcap=10.0, slope0=1e6, mode=MODE_GRID)
+    close = 0
+    for k, li in enumerate(pl):
+        lig = gpu_sys["ligs"][li]
+        got = split_record(lig, out[k])
+        p = poses[k]
+        want, _ = oracle64.bfgs(oracle64.ligand(lig), env, dict(coords=p["coords"].astype(np.float64),
+                                                                 center=p["center"].astype(np.float64),
+                                                                 rot_vec=p["rot_vec"].astype(np.float64),
+                                                                 dihedrals=p["dihedrals"].astype(np.float64)), 400, 10.0, 1e6)
+        if abs(got["energy"] - want["energy"]) <= 1e-3:
+            close += 1
+        # the GPU result is a real minimum of the same model: its energy re-scored by the
+        # oracle agrees with the energy the GPU reports
+        e_chk, _, _ = oracle64.e_grad(oracle64.ligand(lig), env, got["coords"].astype(np.float64),
+                                      got["center"].astype(np.float64), got["rot_vec"].astype(np.float64), vcap=10.0)
+        assert abs(e_chk - got["energy"]) <= 1e-4 * max(1.0, abs(e_chk))
+    frac = close / len(pl)
+    print(f"BFGS same-minimum fraction (|dE| <= 1e-3): {frac:.3f} of {len(pl)}")
+    assert frac >= 0.9
+
+
+def test_bfgs_short_tracks_fp32_oracle(gpu_sys, oracle32):
+    """Two BFGS steps (the refinement unit) match the FP32 oracle closely."""
+    from ud2b200 import MODE_GRID, split_record
+    eng = gpu_sys["eng"]
+    rng = np.random.default_rng(22)
+    env, pl, recs, poses = _starts(gpu_sys, oracle32, rng, 6)
+    out, _ = eng.bfgs_batch(pl, recs, max_steps=2, rounds=1, vcap=1000.0, slope0=1e6, mode=MODE_GRID)
+    bad = 0
+    for k, li in enumerate(pl):
+        lig = gpu_sys["ligs"][li]
+        got = split_record(lig, out[k])
+        p = poses[k]
+        want, _ = oracle32.bfgs(oracle32.ligand(lig), env, dict(coords=p["coords"], center=p["center"],
+                                                                 rot_vec=p["rot_vec"], dihedrals=p["dihedrals"]),
+                                2, 1000.0, 1e6)
+        if abs(got["energy"] - want["energy"]) > 1e-3 * max(1.0, abs(want["energy"])):
+            bad += 1
+    assert bad <= len(pl) // 10
+
+
+def test_search_deterministic(gpu_sys):
+    eng = gpu_sys["eng"]
+    eng.search(seed=42, nchain=16, mc_steps=20, opt_steps=6, randomize=True)
+    a = [eng.chain_poses(l).copy() for l in range(len(gpu_sys["ligs"]))]
+    eng.search(seed=42, nchain=16, mc_steps=20, opt_steps=6, randomize=True)
+    b = [eng.chain_poses(l).copy() for l in range(len(gpu_sys["ligs"]))]
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+def test_search_matches_oracle_chains(gpu_sys, oracle32):
+    """Short MC chains (same counter-based RNG stream) against the FP32 oracle: the best
+    energy of most chains agrees; all GPU best energies are real energies of their poses."""
+    from ud2b200 import split_record
+    from oracle import initial_pose
+    eng = gpu_sys["eng"]
+    nchain, steps, opt = 8, 3, 4
+    eng.search(seed=7, nchain=nchain, mc_steps=steps, opt_steps=opt, randomize=True)
+    env = oracle32.make_env(gpu_sys["rec"], gpu_sys["box"], grid=gpu_sys["ogrid"], mode="grid")
+    agree = total = 0
+    for li, lig in enumerate(gpu_sys["ligs"]):
+        recs = eng.chain_poses(li)
+        olig = oracle32.ligand(lig)
+        for c in range(nchain):
+            got = split_record(lig, recs[c])
+            want, _ = oracle32.mc_chain(olig, env, initial_pose(lig), seed=7, lig_uid=li, chain=c, nchain=nchain,
+                                        mc_steps=steps, opt_steps=opt, randomize=True)
+            total += 1
+            agree += abs(got["energy"] - want["energy"]) <= 1e-3 * max(1.0, abs(want["energy"]))
+    print(f"MC chains agreeing with the FP32 oracle: {agree}/{total}")
+    assert agree >= 0.75 * total
+
+
+def test_randomize_matches_oracle(gpu_sys, oracle64):
+    """mc_steps=0: the chain's pose is the randomised start, scored with curl 10."""
+    from ud2b200 import split_record
+    from oracle import initial_pose
+    eng = gpu_sys["eng"]
+    eng.search(seed=99, nchain=8, mc_steps=0, opt_steps=0, randomize=True)
+    env = oracle64.make_env(gpu_sys["rec"], gpu_sys["box"], grid=gpu_sys["ogrid"], mode="grid")
+    for li, lig in enumerate(gpu_sys["ligs"]):
+        recs = eng.chain_poses(li)
+        for c in range(8):
+            got = split_record(lig, recs[c])
+            want = oracle64.randomize(oracle64.ligand(lig), env, initial_pose(lig), 99, li, c, 8)
+            assert np.allclose(got["coords"], want["coords"], atol=2e-3), (li, c)
+
+
+def test_cluster_bit_exact(gpu_sys, oracle64):
+    eng = gpu_sys["eng"]
+    eng.search(seed=5, nchain=64, mc_steps=10, opt_steps=4, randomize=True)
+    for limit in (0.5, 1.0, 2.0):
+        lead, cnt = eng.cluster(limit)
+        for li, lig in enumerate(gpu_sys["ligs"]):
+            recs = eng.chain_poses(li)
+            n = lig.natom
+            coords = np.ascontiguousarray(recs[:, 8:8 + 3 * n])
+            want = oracle64.cluster(lig.types, coords, recs[:, 0].copy(), limit)
+            assert lead[li, :cnt[li]].tolist() == want
+
+
+def test_dock_end_to_end(gpu_sys, oracle64):
+    from ud2b200 import split_record
+    eng = gpu_sys["eng"]
+    res, ne = eng.dock(seed=3, nchain=32, mc_steps=15, opt_steps=5, refine_steps=3, num_pose=9, rmsd_limit=1.0,
+                       energy_range=10.0)
+    assert ne > 0
+    env = oracle64.make_env(gpu_sys["rec"], gpu_sys["box"], mode="direct")
+    for li, lig in enumerate(gpu_sys["ligs"]):
+        r = res[li]
+        assert 1 <= len(r.records) <= 9
+        es = [split_record(lig, x)["energy"] for x in r.records]
+        assert es == sorted(es)
+        assert es[-1] <= es[0] + 10.0 + 1e-4
+        for k, rec in enumerate(r.records):
+            want = oracle64.score_terms(oracle64.ligand(lig), env, split_record(lig, rec)["coords"].astype(np.float64))
+            assert np.allclose(r.terms[k], want, rtol=1e-4, atol=1e-4)

@@ -1,0 +1,1338 @@
+// ud_engine.cu -- kernels and C ABI of the B200 docking engine (libudock_b200.so).
+//
+// Kernels (all sm_100a, one warp per pose unless noted):
+//   k_grid_build   thread per grid point: per-type Vina maps (new; no reference counterpart)
+//   k_score        E + generalised gradient of a pose batch   (src/cuda/bfgs_wrapper.cu:51-98)
+//   k_terms        final score terms, no curl                 (src/score/score.cpp:12-147)
+//   k_bfgs         BFGS / refinement rounds on pose records   (src/cuda/optimize.cu:14-77)
+//   k_search       persistent MC search: CTA per ligand, warp per chain, chains of a
+//                  ligand handed out from a shared counter    (src/cuda/mc.cu:109-448)
+//   k_cluster      CTA per ligand: energy ranking + greedy RMSD leaders (src/cuda/cluster.cu)
+//   k_filter       CTA per ligand: energy_range / num_pose filter (src/task/DockTask.cpp:188-220)
+// Host orchestration replaces DockTask::run (src/task/DockTask.cpp:39-123).
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+#include <stdexcept>
+#include "ud_device.cuh"
+#include "../../include/udock_b200.h"
+
+using namespace ud;
+
+// ====================================================================== layout helpers
+__host__ __device__ inline int r4(int x) { return (x + 3) & ~3; }
+__host__ __device__ inline int rec_floats(int n, int t) { return r4(8 + 3 * n + t); }
+__host__ __device__ inline int ws_floats(int n, int t) {
+    int d = 6 + t;
+    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(d * (d + 1));
+}
+
+struct LigDev {
+    int blob_off;
+    int blob_words;
+    int natom, ntors, nheavy;
+    int stride;          // record floats
+    int lig_uid;
+    int pad;
+    long long best_off;  // float offset of chain 0's record in the chain-pose buffer
+    long long out_off;   // float offset of the output records (num_pose capacity)
+};
+
+__device__ __forceinline__ Work work_at(float* ws, int natom, int ntors) {
+    int d = 6 + ntors;
+    Work W;
+    W.F = ws + 4 * rec_floats(natom, ntors);
+    W.g = W.F + r4(3 * natom);
+    W.gn = W.g + r4(d);
+    W.p = W.gn + r4(d);
+    W.y = W.p + r4(d);
+    W.mhy = W.y + r4(d);
+    W.H = reinterpret_cast<double*>(W.mhy + r4(d));
+    return W;
+}
+
+__device__ __forceinline__ void copy_words(float* dst, const float* src, int n) {
+    for (int i = lane_id(); i < n; i += WARP) dst[i] = src[i];
+    __syncwarp();
+}
+
+// initial pose from the blob: input coordinates, dihedrals, centre = mean, rot_vec = 0,
+// energy 999 (src/cuda/task.cu:87-105)
+__device__ void load_initial(const int* blob, Slot P, int natom, int ntors) {
+    const float* x0 = reinterpret_cast<const float*>(blob + blob[H_X0]);
+    const float* d0 = reinterpret_cast<const float*>(blob + blob[H_D0]);
+    const float* c0 = reinterpret_cast<const float*>(blob + blob[H_C0]);
+    int lane = lane_id();
+    if (lane == 0) {
+        P.h[0] = 999.f;
+        P.h[1] = c0[0]; P.h[2] = c0[1]; P.h[3] = c0[2];
+        P.h[4] = P.h[5] = P.h[6] = P.h[7] = 0.f;
+    }
+    for (int i = lane; i < 3 * natom; i += WARP) P.x[i] = x0[i];
+    for (int i = lane; i < ntors; i += WARP) P.d[i] = d0[i];
+    __syncwarp();
+}
+
+// ====================================================================== grid build
+__device__ __forceinline__ float eval_e(float d, int t1, int t2) {
+    float f;
+    return eval_ef(d, t1, t2, f);
+}
+
+constexpr int MAX_MAPS = 20;   // every non-hydrogen XS type
+struct MapTypes { int n; int t[MAX_MAPS]; };
+
+__global__ void __launch_bounds__(256) k_grid_build(const float4* __restrict__ rec, int nrec, MapTypes mt,
+                                                    float ox, float oy, float oz, float s, int gx, int gy, int gz,
+                                                    float* __restrict__ out32, __half* __restrict__ out16) {
+    __shared__ float4 tile[256];
+    long long npt = (long long)gx * gy * gz;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int ix = (int)(idx % gx), iy = (int)((idx / gx) % gy), iz = (int)(idx / ((long long)gx * gy));
+    float px = ox + ix * s, py = oy + iy * s, pz = oz + iz * s;
+    float acc[MAX_MAPS];
+    float rm[MAX_MAPS];
+#pragma unroll
+    for (int m = 0; m < MAX_MAPS; m++) { acc[m] = 0.f; rm[m] = m < mt.n ? vdw(mt.t[m]) : 0.f; }
+    for (int base = 0; base < nrec; base += 256) {
+        int j = base + threadIdx.x;
+        if (j < nrec) tile[threadIdx.x] = rec[j];
+        __syncthreads();
+        int nt = min(256, nrec - base);
+        if (idx < npt) {
+            for (int k = 0; k < nt; k++) {
+                float4 r = tile[k];
+                float dx = r.x - px, dy = r.y - py, dz = r.z - pz;
+                float rr = dx * dx + dy * dy + dz * dz;
+                if (rr < 64.f) {
+                    float rn = sqrtf(rr);
+                    int tj = (int)r.w;
+                    float rj = vdw(tj);
+#pragma unroll
+                    for (int m = 0; m < MAX_MAPS; m++)
+                        if (m < mt.n) acc[m] += eval_e(rn - (rm[m] + rj), mt.t[m], tj);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (idx < npt) {
+#pragma unroll
+        for (int m = 0; m < MAX_MAPS; m++) {
+            if (m < mt.n) {
+                out32[(long long)m * npt + idx] = acc[m];
+                if (out16) out16[(long long)m * npt + idx] = __float2half_rn(acc[m]);
+            }
+        }
+    }
+}
+
+// ====================================================================== scoring kernels
+struct PoseIO {
+    const int* lig;          // per pose
+    const long long* xoff;   // per pose: float offset of coords in xyz
+    const float* xyz;
+    const float* centers;    // 3 per pose
+    const float* rotvecs;    // 3 per pose
+    const long long* goff;   // per pose: offset of gradient in out_g
+};
+
+__global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int n, PoseIO io, Env env,
+                        float vcap, float slope, int ws_max, float* out_e, float* out_g) {
+    extern __shared__ __align__(16) float smem[];
+    int warp = threadIdx.x >> 5, lane = lane_id();
+    int pose = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (pose >= n) return;
+    float* ws = smem + (size_t)warp * ws_max;
+    const LigDev L = ligs[io.lig[pose]];
+    const int* blob = blobs + L.blob_off;
+    Topo T = topo_view(blob);
+    Slot P = slot_at(ws, L.stride, 0, T.natom);
+    Work W = work_at(ws, T.natom, T.ntors);
+    const float* x = io.xyz + io.xoff[pose];
+    for (int i = lane; i < 3 * T.natom; i += WARP) P.x[i] = x[i];
+    if (lane < 3) { P.h[1 + lane] = io.centers[3 * pose + lane]; P.h[4 + lane] = io.rotvecs[3 * pose + lane]; }
+    __syncwarp();
+    float e = eval_e_grad(T, env, P, W.F, W.g, vcap, slope);
+    if (lane == 0) out_e[pose] = e;
+    float* g = out_g + io.goff[pose];
+    for (int i = lane; i < 6 + T.ntors; i += WARP) g[i] = W.g[i];
+}
+
+// score() without curl: intra over i<j, inter, penalty (slope 1e6), bias (score.cpp:12-108);
+// decomp = per-atom inter terms (score.cpp:115-147)
+__global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int n, const int* pose_lig,
+                        const long long* xoff, const float* xyz, Env env, float* out4, float* decomp,
+                        const long long* doff) {
+    int warp = threadIdx.x >> 5, lane = lane_id();
+    int pose = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (pose >= n) return;
+    const LigDev L = ligs[pose_lig[pose]];
+    Topo T = topo_view(blobs + L.blob_off);
+    const float* X = xyz + xoff[pose];
+    float e_intra = 0.f, e_inter = 0.f, e_pen = 0.f, e_bias = 0.f;
+    for (int i = lane; i < T.natom; i += WARP) {
+        int ti = T.types[i];
+        float xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
+        for (int k = T.pair_off[i]; k < T.pair_off[i + 1]; k++) {
+            int j = T.pairs[k];
+            if (j <= i) continue;
+            float d0 = X[3 * j] - xi, d1 = X[3 * j + 1] - yi, d2 = X[3 * j + 2] - zi;
+            float rr = d0 * d0 + d1 * d1 + d2 * d2;
+            if (rr < 64.f) e_intra += eval_e(sqrtf(rr) - (vdw(ti) + vdw(T.types[j])), ti, T.types[j]);
+        }
+        if (ti == VN_H) continue;
+        float dec[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+        if (env.mode == 1) {
+            int m = env.map_of_type[ti];
+            float gx, gy, gz;
+            if (m >= 0) e_inter += grid_sample(env.grid, m, xi, yi, zi, gx, gy, gz);
+        } else {
+            for (int j = 0; j < env.nrec; j++) {
+                float4 r = __ldg(env.rec + j);
+                float d0 = r.x - xi, d1 = r.y - yi, d2 = r.z - zi;
+                float rr = d0 * d0 + d1 * d1 + d2 * d2;
+                if (rr < 64.f) {
+                    int tj = (int)r.w;
+                    float d = sqrtf(rr) - (vdw(ti) + vdw(tj));
+                    e_inter += eval_e(d, ti, tj);
+                    if (decomp) {
+                        float x1 = d * 2.f, x2 = (d - 3.f) * 0.5f;
+                        dec[0] += -0.035579f * __expf(-x1 * x1);
+                        dec[1] += -0.005156f * __expf(-x2 * x2);
+                        dec[2] += d < 0.f ? 0.840245f * d * d : 0.f;
+                        unsigned b1 = 1u << ti, b2 = 1u << tj;
+                        if ((b1 & HYD_MASK) && (b2 & HYD_MASK))
+                            dec[3] += -0.035069f * (d <= 0.5f ? 1.f : (d >= 1.5f ? 0.f : 1.5f - d));
+                        if (((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK)))
+                            dec[4] += -0.587439f * (d <= -0.7f ? 1.f : (d >= 0.f ? 0.f : -d / 0.7f));
+                    }
+                }
+            }
+        }
+        if (decomp) {
+            float* o = decomp + doff[pose] + 5 * i;
+            for (int q = 0; q < 5; q++) o[q] = dec[q];
+        }
+        float pen = 0.f;
+        if (xi < env.box_lo[0]) pen += env.box_lo[0] - xi;
+        if (xi > env.box_hi[0]) pen += xi - env.box_hi[0];
+        if (yi < env.box_lo[1]) pen += env.box_lo[1] - yi;
+        if (yi > env.box_hi[1]) pen += yi - env.box_hi[1];
+        if (zi < env.box_lo[2]) pen += env.box_lo[2] - zi;
+        if (zi > env.box_hi[2]) pen += zi - env.box_hi[2];
+        e_pen += pen * PENALTY_SLOPE;
+    }
+    if (decomp) {  // hydrogens get zero rows
+        for (int i = lane; i < T.natom; i += WARP)
+            if (T.types[i] == VN_H)
+                for (int q = 0; q < 5; q++) decomp[doff[pose] + 5 * i + q] = 0.f;
+    }
+    if (env.bias_type != 0) {
+        for (int i = lane; i < T.natom; i += WARP) {
+            for (int b = T.bias_off[i]; b < T.bias_off[i + 1]; b++) {
+                const float* bp = T.bias + 5 * b;
+                float r[3] = {bp[0] - X[3 * i], bp[1] - X[3 * i + 1], bp[2] - X[3 * i + 2]};
+                if (env.bias_type == 1) {
+                    float rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                    e_bias += bp[3] * env.bias_k * expf(-rr / bp[4]);
+                } else {
+                    float ka = T.types[i] == VN_H ? 0.1f : 30.f;
+                    float rn = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                    float ei = expf(3.f * (1.f - rn));
+                    e_bias += bp[3] * env.bias_k * ka / (1.f + ei);
+                }
+            }
+        }
+    }
+    e_intra = warp_sum(e_intra);
+    e_inter = warp_sum(e_inter);
+    e_pen = warp_sum(e_pen);
+    e_bias = warp_sum(e_bias);
+    if (lane == 0) {
+        out4[4 * pose] = e_intra; out4[4 * pose + 1] = e_inter;
+        out4[4 * pose + 2] = e_pen; out4[4 * pose + 3] = e_bias;
+    }
+}
+
+// ====================================================================== BFGS batch
+__global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int n, const int* item_lig,
+                       const long long* item_off, float* recs, Env env, int max_steps, int rounds, float vcap,
+                       float slope0, int ramp, int ws_max, int* nevals) {
+    extern __shared__ __align__(16) float smem[];
+    int warp = threadIdx.x >> 5, lane = lane_id();
+    int item = blockIdx.x * (blockDim.x >> 5) + warp;
+    if (item >= n) return;
+    float* ws = smem + (size_t)warp * ws_max;
+    const LigDev L = ligs[item_lig[item]];
+    Topo T = topo_view(blobs + L.blob_off);
+    Work W = work_at(ws, T.natom, T.ntors);
+    float* rec = recs + item_off[item];
+    int nrec = 8 + 3 * T.natom + T.ntors;
+    copy_words(ws, rec, nrec);
+    int cur = 0, ne = 0;
+    float slope = slope0;
+    for (int r = 0; r < rounds; r++) {
+        int others[3], k = 0;
+        for (int s = 0; s < 4; s++) if (s != cur) others[k++] = s;
+        cur = bfgs(T, env, ws, L.stride, cur, others[0], others[1], W, max_steps, vcap, slope, ne);
+        if (ramp) slope = fminf(slope * 100.f, PENALTY_SLOPE);
+    }
+    copy_words(rec, ws + (size_t)cur * L.stride, nrec);
+    if (nevals && lane == 0) nevals[item] = ne;
+}
+
+// ====================================================================== MC search
+struct SearchP {
+    uint32_t k0, k1;
+    int nchain, mc_steps, opt_steps, randomize;
+    int ws_max;        // floats per warp
+    int blob_max;      // words reserved for the blob
+};
+
+__device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp, float rx) {  // mc.h:12-18
+    if (e_new < e_old) return true;
+    return rx < expf((e_old - e_new) / temp);
+}
+
+__device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
+
+__global__ void __launch_bounds__(256) k_search(const int* __restrict__ blobs, const LigDev* __restrict__ ligs,
+                                                const int* __restrict__ order, int nlig, Env env, SearchP sp,
+                                                float* best, int* work_counter, unsigned long long* nevals) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ int s_lig, s_next;
+    int* sblob = reinterpret_cast<int*>(smem);
+    float* wsbase = smem + sp.blob_max;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    float* ws = wsbase + (size_t)warp * sp.ws_max;
+    unsigned long long my_evals = 0;
+    while (true) {
+        if (threadIdx.x == 0) { s_lig = atomicAdd(work_counter, 1); s_next = 0; }
+        __syncthreads();
+        int li = s_lig;
+        if (li >= nlig) break;
+        const LigDev L = ligs[order[li]];
+        for (int w = threadIdx.x; w < L.blob_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+        __syncthreads();
+        const Topo T = topo_view(sblob);
+        const int nrec = 8 + 3 * T.natom + T.ntors;
+        const Work W = work_at(ws, T.natom, T.ntors);
+        while (true) {
+            int c = 0;
+            if (lane == 0) c = atomicAdd(&s_next, 1);
+            c = __shfl_sync(FULL, c, 0);
+            if (c >= sp.nchain) break;
+            float* out = best + L.best_off + (long long)c * L.stride;
+            Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
+            int A = 0;
+            Slot SA = slot_at(ws, L.stride, A, T.natom);
+            load_initial(sblob, SA, T.natom, T.ntors);
+            if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g);
+            int ne = 0;
+            float best_e = 1e9f;
+            if (sp.mc_steps == 0) {
+                float e = eval_e_f(T, env, SA.x, W.F, VCAP_SEARCH, PENALTY_SLOPE);
+                ne++;
+                if (lane == 0) SA.h[0] = e;
+                __syncwarp();
+                store_record(out, SA, nrec);
+            } else {
+                for (int step = 0; step < sp.mc_steps; step++) {
+                    int fr[3], k = 0;
+                    for (int s = 0; s < 4; s++) if (s != A) fr[k++] = s;
+                    Slot SC = slot_at(ws, L.stride, fr[0], T.natom);
+                    slot_copy(SC, slot_at(ws, L.stride, A, T.natom), T.natom, T.ntors);
+                    mutate(T, env, rng, (uint32_t)step, SC);
+                    int R = fr[0];
+                    if (sp.opt_steps == 0) {
+                        float e = eval_e_grad(T, env, SC, W.F, W.g, VCAP_SEARCH, PENALTY_SLOPE);
+                        ne++;
+                        if (lane == 0) SC.h[0] = e;
+                        __syncwarp();
+                    } else {
+                        R = bfgs(T, env, ws, L.stride, fr[0], fr[1], fr[2], W, sp.opt_steps, VCAP_SEARCH,
+                                 PENALTY_SLOPE, ne);
+                    }
+                    float e_acc = ws[(size_t)A * L.stride];
+                    float e_new = ws[(size_t)R * L.stride];
+                    U4 u = rng.draw((uint32_t)step, P_METRO);
+                    bool acc = metropolis(e_acc, e_new, 1.2f, u01(u.x));
+                    if (step == 0 || acc) {
+                        A = R;
+                        if (e_new < best_e) {
+                            if (sp.opt_steps > 0) {
+                                int g3[3], q = 0;
+                                for (int s = 0; s < 4; s++) if (s != A) g3[q++] = s;
+                                A = bfgs(T, env, ws, L.stride, A, g3[0], g3[1], W, sp.opt_steps, VCAP_AUTH,
+                                         PENALTY_SLOPE, ne);
+                            }
+                            float ea = ws[(size_t)A * L.stride];
+                            if (ea < best_e) {
+                                best_e = ea;
+                                store_record(out, slot_at(ws, L.stride, A, T.natom), nrec);
+                            }
+                        }
+                    }
+                }
+            }
+            my_evals += ne;
+        }
+        __syncthreads();
+    }
+    if (lane == 0 && nevals) atomicAdd(nevals, my_evals);
+}
+
+// ====================================================================== clustering
+// CTA per ligand.  Ranking by (energy, index) with NaN as +inf; greedy leaders with
+// per-thread fixed-order fmaf sums over heavy atoms (bit-identical to the oracle).
+__global__ void k_cluster(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int nlig, int nchain,
+                          const float* __restrict__ best, float rmsd_limit, int* leaders, int* counts) {
+    extern __shared__ __align__(16) float smem[];
+    float* e = smem;
+    int* order = reinterpret_cast<int*>(e + nchain);
+    int* lead = order + nchain;
+    __shared__ int s_nl;
+    int lig = blockIdx.x;
+    if (lig >= nlig) return;
+    const LigDev L = ligs[lig];
+    Topo T = topo_view(blobs + L.blob_off);
+    const float* base = best + L.best_off;
+    for (int i = threadIdx.x; i < nchain; i += blockDim.x) {
+        float v = base[(long long)i * L.stride];
+        e[i] = isnan(v) ? INFINITY : v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nchain; i += blockDim.x) {
+        float ei = e[i];
+        int r = 0;
+        for (int j = 0; j < nchain; j++) {
+            float ej = e[j];
+            r += (ej < ei) || (ej == ei && j < i);
+        }
+        order[r] = i;
+    }
+    if (threadIdx.x == 0) s_nl = 0;
+    __syncthreads();
+    float thr = __fmul_rn(__fmul_rn(rmsd_limit, rmsd_limit), (float)T.nheavy);
+    for (int o = 0; o < nchain; o++) {
+        int c = order[o];
+        int nl = s_nl;
+        const float* xc = base + (long long)c * L.stride + 8;
+        int close = 0;
+        for (int t = threadIdx.x; t < nl; t += blockDim.x) {
+            const float* xl = base + (long long)lead[t] * L.stride + 8;
+            float acc = 0.f;
+            for (int h = 0; h < T.nheavy; h++) {
+                int a = T.heavy[h];
+                float dx = __fsub_rn(xc[3 * a], xl[3 * a]);
+                float dy = __fsub_rn(xc[3 * a + 1], xl[3 * a + 1]);
+                float dz = __fsub_rn(xc[3 * a + 2], xl[3 * a + 2]);
+                acc = __fmaf_rn(dx, dx, acc);
+                acc = __fmaf_rn(dy, dy, acc);
+                acc = __fmaf_rn(dz, dz, acc);
+            }
+            if (acc < thr) close = 1;
+        }
+        int any = __syncthreads_or(close);
+        if (!any && threadIdx.x == 0) { lead[nl] = c; s_nl = nl + 1; }
+        __syncthreads();
+    }
+    int nl = s_nl;
+    for (int i = threadIdx.x; i < nchain; i += blockDim.x) leaders[(long long)lig * nchain + i] = i < nl ? lead[i] : -1;
+    if (threadIdx.x == 0) counts[lig] = nl;
+}
+
+// energy_range / num_pose filter over the refined leaders (DockTask.cpp:188-220);
+// out_sel[lig*num_pose + k] = chain index of the k-th output pose
+__global__ void k_filter(const LigDev* __restrict__ ligs, int nlig, int nchain, const float* __restrict__ best,
+                         const int* leaders, const int* counts, int num_pose, float energy_range, int* out_sel,
+                         int* out_count) {
+    extern __shared__ __align__(16) float smem[];
+    float* e = smem;
+    int* order = reinterpret_cast<int*>(e + nchain);
+    int lig = blockIdx.x;
+    if (lig >= nlig) return;
+    const LigDev L = ligs[lig];
+    int nl = counts[lig];
+    const int* ld = leaders + (long long)lig * nchain;
+    for (int i = threadIdx.x; i < nl; i += blockDim.x) {
+        float v = best[L.best_off + (long long)ld[i] * L.stride];
+        e[i] = isnan(v) ? INFINITY : v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nl; i += blockDim.x) {
+        float ei = e[i];
+        int r = 0;
+        for (int j = 0; j < nl; j++) r += (e[j] < ei) || (e[j] == ei && j < i);
+        order[r] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int cnt = 0;
+        if (nl > 0) {
+            float emin = e[order[0]];
+            for (int k = 0; k < nl; k++) {
+                float v = e[order[k]];
+                if (v > emin + energy_range) break;
+                out_sel[(long long)lig * num_pose + cnt] = ld[order[k]];
+                cnt++;
+                if (cnt >= num_pose) break;
+            }
+        }
+        out_count[lig] = cnt;
+    }
+}
+
+// gather selected records into the output buffer and list them for scoring
+__global__ void k_gather(const LigDev* __restrict__ ligs, int nlig, int num_pose, const float* __restrict__ best,
+                         const int* sel, const int* cnt, float* out_rec) {
+    int warp = threadIdx.x >> 5;
+    long long item = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (item >= (long long)nlig * num_pose) return;
+    int lig = (int)(item / num_pose), k = (int)(item % num_pose);
+    if (k >= cnt[lig]) return;
+    const LigDev L = ligs[lig];
+    int c = sel[item];
+    const float* src = best + L.best_off + (long long)c * L.stride;
+    float* dst = out_rec + L.out_off + (long long)k * L.stride;
+    for (int i = lane_id(); i < L.stride; i += WARP) dst[i] = src[i];
+}
+
+// ====================================================================== host side
+namespace {
+thread_local std::string g_err;
+
+struct Fail : std::runtime_error {
+    int code;
+    Fail(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw Fail(UD_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (count == 0) count = 1;
+        ck(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        ensure(count);
+        if (count) ck(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+};
+
+struct LigHost {
+    int natom, ntors, nheavy, blob_words, stride;
+    long long blob_off;
+};
+}  // namespace
+
+struct ud_ctx {
+    int device = 0;
+    int nsm = 148;
+    cudaStream_t stream = nullptr;
+    float box_lo[3], box_hi[3];
+    int constraint = 0, bias_type = 0;
+    float bias_k = 0.1f;
+    // receptor
+    std::vector<float4> h_rec;
+    DBuf<float4> d_rec;
+    // grid
+    DBuf<float> d_maps32;
+    DBuf<__half> d_maps16;
+    int nmaps = 0, gdim[3] = {0, 0, 0}, grid_prec = 0;
+    float origin[3] = {0, 0, 0}, spacing = 0.f;
+    signed char map_of_type[NT + 3];
+    // ligands
+    std::vector<int> h_blobs;
+    std::vector<LigHost> h_ligs;
+    std::vector<LigDev> h_ligdev;
+    DBuf<int> d_blobs;
+    DBuf<LigDev> d_ligs;
+    bool ligs_dirty = true;
+    int max_natom = 0, max_ntors = 0, max_blob = 0;
+    // search state
+    int nchain = 0;
+    long long best_floats = 0;
+    DBuf<float> d_best;
+    DBuf<int> d_order, d_counter, d_leaders, d_counts, d_sel, d_selcnt;
+    DBuf<unsigned long long> d_nevals;
+    // results
+    int num_pose = 0;
+    long long out_floats = 0;
+    DBuf<float> d_out, d_terms, d_decomp;
+    DBuf<int> d_item_lig;
+    DBuf<long long> d_item_off, d_item_off2;
+    std::vector<int> h_counts;
+    bool has_results = false;
+    bool decomp = false;
+};
+
+namespace {
+
+int fail(const Fail& f) {
+    g_err = f.what();
+    return f.code;
+}
+
+Env make_env(ud_ctx* c, int mode) {
+    Env e;
+    for (int a = 0; a < 3; a++) { e.box_lo[a] = c->box_lo[a]; e.box_hi[a] = c->box_hi[a]; }
+    e.mode = mode;
+    e.constraint = c->constraint;
+    e.bias_type = c->bias_type;
+    e.bias_k = c->bias_k;
+    e.rec = c->d_rec.p;
+    e.nrec = (int)c->h_rec.size();
+    e.grid.f32 = c->d_maps32.p;
+    e.grid.f16 = c->d_maps16.p;
+    e.grid.use_f16 = (c->grid_prec == UD_GRID_F16 && c->d_maps16.p) ? 1 : 0;
+    e.grid.ox = c->origin[0]; e.grid.oy = c->origin[1]; e.grid.oz = c->origin[2];
+    e.grid.inv_s = c->spacing > 0 ? 1.f / c->spacing : 0.f;
+    e.grid.gx = c->gdim[0]; e.grid.gy = c->gdim[1]; e.grid.gz = c->gdim[2];
+    memcpy(e.map_of_type, c->map_of_type, sizeof(e.map_of_type));
+    if (mode == UD_MODE_GRID && c->nmaps == 0) throw Fail(UD_ESTATE, "grid mode requested but no grid was built");
+    return e;
+}
+
+void sync_ligs(ud_ctx* c) {
+    if (!c->ligs_dirty) return;
+    c->d_blobs.upload(c->h_blobs.data(), c->h_blobs.size(), c->stream);
+    c->h_ligdev.resize(c->h_ligs.size());
+    for (size_t i = 0; i < c->h_ligs.size(); i++) {
+        const LigHost& h = c->h_ligs[i];
+        LigDev& d = c->h_ligdev[i];
+        d.blob_off = (int)h.blob_off;
+        d.blob_words = h.blob_words;
+        d.natom = h.natom;
+        d.ntors = h.ntors;
+        d.nheavy = h.nheavy;
+        d.stride = h.stride;
+        d.lig_uid = (int)i;
+        d.pad = 0;
+        d.best_off = 0;
+        d.out_off = 0;
+    }
+    c->d_ligs.upload(c->h_ligdev.data(), c->h_ligdev.size(), c->stream);
+    c->ligs_dirty = false;
+}
+
+void upload_ligdev(ud_ctx* c) { c->d_ligs.upload(c->h_ligdev.data(), c->h_ligdev.size(), c->stream); }
+
+int smem_limit(ud_ctx* c) {
+    int v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    return v > 0 ? v : 48 * 1024;
+}
+
+// warps per CTA so that W warps of ws floats fit beside `extra` floats
+int pick_warps(ud_ctx* c, int ws, int extra, int want) {
+    int lim = smem_limit(c) / 4 - extra - 64;
+    int w = want;
+    while (w > 1 && w * ws > lim) w--;
+    if (w * ws > lim) throw Fail(UD_EINVAL, "ligand too large for shared memory");
+    return w;
+}
+
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+    ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "smem attribute");
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+int ud_version(void) { return 100; }
+
+const char* ud_last_error(void) { return g_err.c_str(); }
+
+int ud_create(int device, const float* box6, ud_ctx** out) {
+    try {
+        if (!out || !box6) throw Fail(UD_EINVAL, "null argument");
+        int ndev = 0;
+        ck(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+        if (ndev <= 0) throw Fail(UD_ECUDA, "No CUDA device is found!");
+        if (device < 0 || device >= ndev) throw Fail(UD_EINVAL, "invalid device id");
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        ud_ctx* c = new ud_ctx();
+        c->device = device;
+        cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+        ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        c->box_lo[0] = box6[0]; c->box_hi[0] = box6[1];
+        c->box_lo[1] = box6[2]; c->box_hi[1] = box6[3];
+        c->box_lo[2] = box6[4]; c->box_hi[2] = box6[5];
+        for (int i = 0; i < NT + 3; i++) c->map_of_type[i] = -1;
+        *out = c;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_destroy(ud_ctx* c) {
+    if (!c) return UD_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->d_rec.release(); c->d_maps32.release(); c->d_maps16.release();
+    c->d_blobs.release(); c->d_ligs.release(); c->d_best.release();
+    c->d_order.release(); c->d_counter.release(); c->d_leaders.release(); c->d_counts.release();
+    c->d_sel.release(); c->d_selcnt.release(); c->d_nevals.release();
+    c->d_out.release(); c->d_terms.release(); c->d_decomp.release();
+    c->d_item_lig.release(); c->d_item_off.release(); c->d_item_off2.release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return UD_OK;
+}
+
+int ud_set_flags(ud_ctx* c, int constraint, int bias_type, float bias_k) {
+    if (!c) { g_err = "null context"; return UD_EINVAL; }
+    if (bias_type < 0 || bias_type > 2) { g_err = "bias_type must be 0, 1 or 2"; return UD_EINVAL; }
+    c->constraint = constraint ? 1 : 0;
+    c->bias_type = bias_type;
+    c->bias_k = bias_k;
+    return UD_OK;
+}
+
+int ud_set_receptor(ud_ctx* c, int n, const float* xyz, const int* types) {
+    try {
+        if (!c || n < 0 || (n > 0 && (!xyz || !types))) throw Fail(UD_EINVAL, "invalid receptor arguments");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        c->h_rec.clear();
+        for (int i = 0; i < n; i++) {
+            int t = types[i];
+            if (t < 0 || t >= NT) throw Fail(UD_EINVAL, "receptor type out of range");
+            if (t == VN_H) continue;
+            float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+            bool in = (c->box_lo[0] - 8.f <= x && x <= c->box_hi[0] + 8.f) &&
+                      (c->box_lo[1] - 8.f <= y && y <= c->box_hi[1] + 8.f) &&
+                      (c->box_lo[2] - 8.f <= z && z <= c->box_hi[2] + 8.f);
+            if (in) c->h_rec.push_back(make_float4(x, y, z, (float)t));
+        }
+        c->d_rec.upload(c->h_rec.data(), c->h_rec.size(), c->stream);
+        ck(cudaStreamSynchronize(c->stream), "receptor upload");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_receptor_count(const ud_ctx* c) { return c ? (int)c->h_rec.size() : 0; }
+
+int ud_build_grid(ud_ctx* c, float spacing, int nmaps, const int* map_types, int precision) {
+    try {
+        if (!c || spacing <= 0.f || nmaps <= 0 || nmaps > MAX_MAPS || !map_types)
+            throw Fail(UD_EINVAL, "invalid grid arguments (1..20 maps, spacing > 0)");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        MapTypes mt;
+        mt.n = nmaps;
+        for (int i = 0; i < NT + 3; i++) c->map_of_type[i] = -1;
+        for (int m = 0; m < nmaps; m++) {
+            if (map_types[m] <= 0 || map_types[m] >= NT) throw Fail(UD_EINVAL, "map type out of range");
+            mt.t[m] = map_types[m];
+            c->map_of_type[map_types[m]] = (signed char)m;
+        }
+        for (int a = 0; a < 3; a++) {
+            c->origin[a] = c->box_lo[a];
+            c->gdim[a] = (int)ceilf((c->box_hi[a] - c->box_lo[a]) / spacing - 1e-4f) + 1;
+            if (c->gdim[a] < 2) c->gdim[a] = 2;
+        }
+        c->spacing = spacing;
+        c->nmaps = nmaps;
+        long long npt = (long long)c->gdim[0] * c->gdim[1] * c->gdim[2];
+        c->d_maps32.ensure((size_t)npt * nmaps);
+        c->d_maps16.ensure((size_t)npt * nmaps);
+        int threads = 256;
+        long long blocks = (npt + threads - 1) / threads;
+        k_grid_build<<<(unsigned)blocks, threads, 0, c->stream>>>(c->d_rec.p, (int)c->h_rec.size(), mt, c->origin[0],
+                                                                  c->origin[1], c->origin[2], spacing, c->gdim[0],
+                                                                  c->gdim[1], c->gdim[2], c->d_maps32.p, c->d_maps16.p);
+        ck(cudaGetLastError(), "k_grid_build launch");
+        ck(cudaStreamSynchronize(c->stream), "k_grid_build");
+        c->grid_prec = precision == UD_GRID_F16 ? UD_GRID_F16 : UD_GRID_F32;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_set_grid_precision(ud_ctx* c, int precision) {
+    if (!c) { g_err = "null context"; return UD_EINVAL; }
+    c->grid_prec = precision == UD_GRID_F16 ? UD_GRID_F16 : UD_GRID_F32;
+    return UD_OK;
+}
+
+int ud_get_grid(const ud_ctx* c, float* out, int* gdim3, float* origin3) {
+    try {
+        if (!c || c->nmaps == 0) throw Fail(UD_ESTATE, "no grid built");
+        if (gdim3) for (int a = 0; a < 3; a++) gdim3[a] = c->gdim[a];
+        if (origin3) for (int a = 0; a < 3; a++) origin3[a] = c->origin[a];
+        if (out) {
+            ck(cudaSetDevice(c->device), "cudaSetDevice");
+            size_t n = (size_t)c->gdim[0] * c->gdim[1] * c->gdim[2] * c->nmaps;
+            ck(cudaMemcpy(out, c->d_maps32.p, n * sizeof(float), cudaMemcpyDeviceToHost), "grid D2H");
+        }
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, const int* types, const int* tors_off,
+                   const int* axis, const float* dihedrals, const int* range_off, const float* ranges,
+                   const int* rot_off, const int* rot_atoms, const int* pair_off, const int* pairs,
+                   const int* bias_off, const float* bias) {
+    try {
+        if (!c || nlig < 0 || !atom_off || !tors_off || !range_off || !rot_off || !pair_off)
+            throw Fail(UD_EINVAL, "invalid ligand arguments");
+        for (int l = 0; l < nlig; l++) {
+            int a0 = atom_off[l], n = atom_off[l + 1] - a0;
+            int t0 = tors_off[l], T = tors_off[l + 1] - t0;
+            if (n <= 0 || T < 0) throw Fail(UD_EINVAL, "ligand with no atoms");
+            if (n > 4096 || T > 256) throw Fail(UD_EINVAL, "ligand too large (max 4096 atoms, 256 torsions)");
+            int nheavy = 0;
+            for (int i = 0; i < n; i++) {
+                int t = types[a0 + i];
+                if (t < 0 || t >= NT) throw Fail(UD_EINVAL, "ligand atom type out of range");
+                nheavy += t != VN_H;
+            }
+            int p0 = pair_off[a0], np = pair_off[a0 + n] - p0;
+            int r0 = rot_off[t0], nrot = rot_off[t0 + T] - r0;
+            int g0 = range_off[t0], nrange = range_off[t0 + T] - g0;
+            int b0 = bias_off ? bias_off[a0] : 0, nb = bias_off ? bias_off[a0 + n] - b0 : 0;
+            std::vector<int> blob(H_WORDS, 0);
+            auto put = [&](int hdr, int count) {
+                blob[hdr] = (int)blob.size();
+                blob.resize(blob.size() + ((count + 3) & ~3), 0);
+                return blob[hdr];
+            };
+            blob[H_NATOM] = n; blob[H_NTORS] = T; blob[H_NHEAVY] = nheavy; blob[H_NPAIR] = np;
+            blob[H_NROT] = nrot; blob[H_NRANGE] = nrange; blob[H_NBIAS] = nb;
+            int o;
+            o = put(H_TYPES, n);
+            for (int i = 0; i < n; i++) blob[o + i] = types[a0 + i];
+            o = put(H_AXIS, 2 * T);
+            for (int k = 0; k < 2 * T; k++) {
+                int v = axis[2 * t0 + k];
+                if (v < 0 || v >= n) throw Fail(UD_EINVAL, "torsion axis atom out of range");
+                blob[o + k] = v;
+            }
+            o = put(H_RANGE_OFF, T + 1);
+            for (int k = 0; k <= T; k++) blob[o + k] = range_off[t0 + k] - g0;
+            for (int k = 0; k < T; k++)
+                if (range_off[t0 + k + 1] - range_off[t0 + k] <= 0) throw Fail(UD_EINVAL, "torsion without range");
+            o = put(H_RANGES, 2 * nrange);
+            memcpy(&blob[o], ranges + 2 * (size_t)g0, sizeof(float) * 2 * nrange);
+            o = put(H_ROT_OFF, T + 1);
+            for (int k = 0; k <= T; k++) blob[o + k] = rot_off[t0 + k] - r0;
+            o = put(H_ROT, nrot);
+            for (int k = 0; k < nrot; k++) {
+                int v = rot_atoms[r0 + k];
+                if (v < 0 || v >= n) throw Fail(UD_EINVAL, "rotated atom out of range");
+                blob[o + k] = v;
+            }
+            o = put(H_PAIR_OFF, n + 1);
+            for (int i = 0; i <= n; i++) blob[o + i] = pair_off[a0 + i] - p0;
+            o = put(H_PAIRS, np);
+            for (int k = 0; k < np; k++) {
+                int v = pairs[p0 + k];
+                if (v < 0 || v >= n) throw Fail(UD_EINVAL, "intra pair atom out of range");
+                blob[o + k] = v;
+            }
+            o = put(H_BIAS_OFF, n + 1);
+            for (int i = 0; i <= n; i++) blob[o + i] = bias_off ? bias_off[a0 + i] - b0 : 0;
+            o = put(H_BIAS, 5 * nb);
+            if (nb) memcpy(&blob[o], bias + 5 * (size_t)b0, sizeof(float) * 5 * nb);
+            o = put(H_HEAVY, nheavy);
+            for (int i = 0, k = 0; i < n; i++) if (types[a0 + i] != VN_H) blob[o + k++] = i;
+            o = put(H_X0, 3 * n);
+            memcpy(&blob[o], xyz + 3 * (size_t)a0, sizeof(float) * 3 * n);
+            o = put(H_D0, T);
+            if (T) memcpy(&blob[o], dihedrals + t0, sizeof(float) * T);
+            o = put(H_C0, 3);
+            {   // centre = float mean of the input coordinates (rapidjson_parser.cpp:67-83,197-199)
+                float s[3] = {0.f, 0.f, 0.f};
+                for (int i = 0; i < n; i++)
+                    for (int a = 0; a < 3; a++) s[a] += xyz[3 * (size_t)(a0 + i) + a];
+                float cc[3] = {s[0] / n, s[1] / n, s[2] / n};
+                memcpy(&blob[o], cc, sizeof(cc));
+            }
+            blob[H_TOTAL] = (int)blob.size();
+            LigHost h;
+            h.natom = n; h.ntors = T; h.nheavy = nheavy;
+            h.blob_words = (int)blob.size();
+            h.blob_off = (long long)c->h_blobs.size();
+            h.stride = rec_floats(n, T);
+            c->h_blobs.insert(c->h_blobs.end(), blob.begin(), blob.end());
+            c->h_ligs.push_back(h);
+            c->max_natom = std::max(c->max_natom, n);
+            c->max_ntors = std::max(c->max_ntors, T);
+            c->max_blob = std::max(c->max_blob, h.blob_words);
+        }
+        c->ligs_dirty = true;
+        c->has_results = false;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_clear_ligands(ud_ctx* c) {
+    if (!c) { g_err = "null context"; return UD_EINVAL; }
+    c->h_blobs.clear();
+    c->h_ligs.clear();
+    c->h_ligdev.clear();
+    c->max_natom = c->max_ntors = c->max_blob = 0;
+    c->ligs_dirty = true;
+    c->has_results = false;
+    c->nchain = 0;
+    return UD_OK;
+}
+
+int ud_ligand_count(const ud_ctx* c) { return c ? (int)c->h_ligs.size() : 0; }
+
+int ud_record_floats(const ud_ctx* c, int lig) {
+    if (!c || lig < 0 || lig >= (int)c->h_ligs.size()) { g_err = "invalid ligand index"; return UD_EINVAL; }
+    return c->h_ligs[lig].stride;
+}
+
+int ud_score_batch(ud_ctx* c, int n, const int* pose_lig, const float* coords, const float* centers,
+                   const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g) {
+    try {
+        if (!c || n < 0 || (n > 0 && (!pose_lig || !coords || !centers || !rotvecs || !out_e || !out_g)))
+            throw Fail(UD_EINVAL, "invalid score arguments");
+        if (n == 0) return UD_OK;
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        sync_ligs(c);
+        Env env = make_env(c, mode);
+        std::vector<long long> xoff(n), goff(n);
+        long long xs = 0, gs = 0;
+        int wsm = 0;
+        for (int i = 0; i < n; i++) {
+            int l = pose_lig[i];
+            if (l < 0 || l >= (int)c->h_ligs.size()) throw Fail(UD_EINVAL, "pose ligand index out of range");
+            xoff[i] = xs;
+            goff[i] = gs;
+            xs += 3LL * c->h_ligs[l].natom;
+            gs += 6 + c->h_ligs[l].ntors;
+            wsm = std::max(wsm, ws_floats(c->h_ligs[l].natom, c->h_ligs[l].ntors));
+        }
+        DBuf<int> dl; DBuf<long long> dxo, dgo; DBuf<float> dx, dc, dr, de, dg;
+        dl.upload(pose_lig, n, c->stream);
+        dxo.upload(xoff.data(), n, c->stream);
+        dgo.upload(goff.data(), n, c->stream);
+        dx.upload(coords, xs, c->stream);
+        dc.upload(centers, 3 * (size_t)n, c->stream);
+        dr.upload(rotvecs, 3 * (size_t)n, c->stream);
+        de.ensure(n);
+        dg.ensure(gs);
+        int W = pick_warps(c, wsm, 0, 8);
+        size_t smem = (size_t)W * wsm * 4;
+        set_smem(k_score, smem);
+        PoseIO io{dl.p, dxo.p, dx.p, dc.p, dr.p, dgo.p};
+        k_score<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm,
+                                                              de.p, dg.p);
+        ck(cudaGetLastError(), "k_score launch");
+        ck(cudaMemcpyAsync(out_e, de.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaMemcpyAsync(out_g, dg.p, gs * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "k_score");
+        for (auto* b : {&dx, &dc, &dr, &de, &dg}) b->release();
+        dl.release(); dxo.release(); dgo.release();
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_score_terms(ud_ctx* c, int n, const int* pose_lig, const float* coords, int mode, float* out4,
+                   float* out_decomp) {
+    try {
+        if (!c || n < 0 || (n > 0 && (!pose_lig || !coords || !out4))) throw Fail(UD_EINVAL, "invalid arguments");
+        if (n == 0) return UD_OK;
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        sync_ligs(c);
+        Env env = make_env(c, mode);
+        std::vector<long long> xoff(n), doff(n);
+        long long xs = 0, ds = 0;
+        for (int i = 0; i < n; i++) {
+            int l = pose_lig[i];
+            if (l < 0 || l >= (int)c->h_ligs.size()) throw Fail(UD_EINVAL, "pose ligand index out of range");
+            xoff[i] = xs;
+            doff[i] = ds;
+            xs += 3LL * c->h_ligs[l].natom;
+            ds += 5LL * c->h_ligs[l].natom;
+        }
+        DBuf<int> dl; DBuf<long long> dxo, ddo; DBuf<float> dx, d4, dd;
+        dl.upload(pose_lig, n, c->stream);
+        dxo.upload(xoff.data(), n, c->stream);
+        ddo.upload(doff.data(), n, c->stream);
+        dx.upload(coords, xs, c->stream);
+        d4.ensure(4 * (size_t)n);
+        if (out_decomp) dd.ensure(ds);
+        int W = 8;
+        k_terms<<<(n + W - 1) / W, 32 * W, 0, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, dl.p, dxo.p, dx.p, env, d4.p,
+                                                           out_decomp ? dd.p : nullptr, ddo.p);
+        ck(cudaGetLastError(), "k_terms launch");
+        ck(cudaMemcpyAsync(out4, d4.p, 4 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        if (out_decomp)
+            ck(cudaMemcpyAsync(out_decomp, dd.p, ds * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "k_terms");
+        dl.release(); dxo.release(); ddo.release(); dx.release(); d4.release(); dd.release();
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_bfgs_batch(ud_ctx* c, int n, const int* pose_lig, float* records, int max_steps, int rounds, float vcap,
+                  float slope0, int ramp, int mode, int* out_nevals) {
+    try {
+        if (!c || n < 0 || (n > 0 && (!pose_lig || !records)) || max_steps < 0 || rounds < 0)
+            throw Fail(UD_EINVAL, "invalid bfgs arguments");
+        if (n == 0) return UD_OK;
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        sync_ligs(c);
+        Env env = make_env(c, mode);
+        std::vector<long long> off(n);
+        long long tot = 0;
+        int wsm = 0;
+        for (int i = 0; i < n; i++) {
+            int l = pose_lig[i];
+            if (l < 0 || l >= (int)c->h_ligs.size()) throw Fail(UD_EINVAL, "pose ligand index out of range");
+            off[i] = tot;
+            tot += c->h_ligs[l].stride;
+            wsm = std::max(wsm, ws_floats(c->h_ligs[l].natom, c->h_ligs[l].ntors));
+        }
+        // records are packed at 8+3N+T floats each on the host side
+        std::vector<float> packed(tot, 0.f);
+        long long hs = 0;
+        for (int i = 0; i < n; i++) {
+            const LigHost& h = c->h_ligs[pose_lig[i]];
+            int nr = 8 + 3 * h.natom + h.ntors;
+            memcpy(&packed[off[i]], records + hs, nr * sizeof(float));
+            hs += nr;
+        }
+        DBuf<int> dl, dn; DBuf<long long> dof; DBuf<float> dr;
+        dl.upload(pose_lig, n, c->stream);
+        dof.upload(off.data(), n, c->stream);
+        dr.upload(packed.data(), tot, c->stream);
+        dn.ensure(n);
+        int W = pick_warps(c, wsm, 0, 8);
+        size_t smem = (size_t)W * wsm * 4;
+        set_smem(k_bfgs, smem);
+        k_bfgs<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, dl.p, dof.p, dr.p, env,
+                                                             max_steps, rounds, vcap, slope0, ramp, wsm, dn.p);
+        ck(cudaGetLastError(), "k_bfgs launch");
+        ck(cudaMemcpyAsync(packed.data(), dr.p, tot * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        if (out_nevals) ck(cudaMemcpyAsync(out_nevals, dn.p, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "k_bfgs");
+        hs = 0;
+        for (int i = 0; i < n; i++) {
+            const LigHost& h = c->h_ligs[pose_lig[i]];
+            int nr = 8 + 3 * h.natom + h.ntors;
+            memcpy(records + hs, &packed[off[i]], nr * sizeof(float));
+            hs += nr;
+        }
+        dl.release(); dn.release(); dof.release(); dr.release();
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode) {
+    sync_ligs(c);
+    Env env = make_env(c, mode);
+    int nlig = (int)c->h_ligs.size();
+    c->nchain = nchain;
+    long long tot = 0;
+    int wsm = 0;
+    std::vector<int> order(nlig);
+    std::vector<double> cost(nlig);
+    for (int l = 0; l < nlig; l++) {
+        const LigHost& h = c->h_ligs[l];
+        c->h_ligdev[l].best_off = tot;
+        tot += (long long)nchain * h.stride;
+        wsm = std::max(wsm, ws_floats(h.natom, h.ntors));
+        order[l] = l;
+        cost[l] = (double)(h.natom + 8) * (6 + h.ntors);   // rough: heavier ligands first
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    upload_ligdev(c);
+    c->best_floats = tot;
+    c->d_best.ensure((size_t)tot);
+    c->d_order.upload(order.data(), nlig, c->stream);
+    c->d_counter.ensure(1);
+    c->d_nevals.ensure(1);
+    ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
+    ck(cudaMemsetAsync(c->d_nevals.p, 0, sizeof(unsigned long long), c->stream), "memset");
+    int blob_max = r4(c->max_blob);
+    int W = pick_warps(c, wsm, blob_max, 8);
+    size_t smem = ((size_t)blob_max + (size_t)W * wsm) * 4;
+    set_smem(k_search, smem);
+    int per_sm = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, 32 * W, smem), "occupancy");
+    if (per_sm < 1) per_sm = 1;
+    int grid = std::min(nlig, c->nsm * per_sm);
+    SearchP sp;
+    sp.k0 = (uint32_t)seed;
+    sp.k1 = (uint32_t)(seed >> 32) ^ 0x5DEECE66u;
+    sp.nchain = nchain;
+    sp.mc_steps = mc_steps;
+    sp.opt_steps = opt_steps;
+    sp.randomize = randomize;
+    sp.ws_max = wsm;
+    sp.blob_max = blob_max;
+    if (grid > 0) {
+        k_search<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_order.p, nlig, env, sp,
+                                                    c->d_best.p, c->d_counter.p, c->d_nevals.p);
+        ck(cudaGetLastError(), "k_search launch");
+    }
+}
+
+int ud_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode,
+              long long* out_nevals) {
+    try {
+        if (!c || nchain <= 0 || mc_steps < 0 || opt_steps < 0) throw Fail(UD_EINVAL, "invalid search arguments");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        launch_search(c, seed, nchain, mc_steps, opt_steps, randomize, mode);
+        unsigned long long ne = 0;
+        ck(cudaMemcpyAsync(&ne, c->d_nevals.p, sizeof(ne), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "k_search");
+        if (out_nevals) *out_nevals = (long long)ne;
+        c->has_results = false;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_get_chain_poses(const ud_ctx* c, int lig, float* out) {
+    try {
+        if (!c || lig < 0 || lig >= (int)c->h_ligs.size() || !out || c->nchain == 0)
+            throw Fail(UD_EINVAL, "invalid arguments or no search results");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        const LigHost& h = c->h_ligs[lig];
+        ck(cudaMemcpy(out, c->d_best.p + c->h_ligdev[lig].best_off, (size_t)c->nchain * h.stride * sizeof(float),
+                      cudaMemcpyDeviceToHost), "D2H");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+static void launch_cluster(ud_ctx* c, float rmsd_limit) {
+    int nlig = (int)c->h_ligs.size();
+    int nchain = c->nchain;
+    c->d_leaders.ensure((size_t)nlig * nchain);
+    c->d_counts.ensure(nlig);
+    size_t smem = (size_t)nchain * 12;
+    set_smem(k_cluster, smem);
+    int threads = std::min(1024, std::max(32, ((nchain + 31) / 32) * 32));
+    k_cluster<<<nlig, threads, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, nlig, nchain, c->d_best.p, rmsd_limit,
+                                                  c->d_leaders.p, c->d_counts.p);
+    ck(cudaGetLastError(), "k_cluster launch");
+}
+
+int ud_cluster(ud_ctx* c, float rmsd_limit, int* out_leaders, int* out_counts) {
+    try {
+        if (!c || c->nchain == 0) throw Fail(UD_ESTATE, "no search results to cluster");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        launch_cluster(c, rmsd_limit);
+        int nlig = (int)c->h_ligs.size();
+        if (out_leaders)
+            ck(cudaMemcpyAsync(out_leaders, c->d_leaders.p, (size_t)nlig * c->nchain * sizeof(int),
+                               cudaMemcpyDeviceToHost, c->stream), "D2H");
+        if (out_counts)
+            ck(cudaMemcpyAsync(out_counts, c->d_counts.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "k_cluster");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
+    try {
+        if (!c || !p || p->nchain <= 0 || p->mc_steps < 0 || p->opt_steps < 0 || p->num_pose <= 0 ||
+            p->refine_steps < 0)
+            throw Fail(UD_EINVAL, "invalid dock parameters");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        int nlig = (int)c->h_ligs.size();
+        if (nlig == 0) throw Fail(UD_ESTATE, "no ligands loaded");
+        launch_search(c, p->seed, p->nchain, p->mc_steps, p->opt_steps, p->randomize, p->mode);
+        launch_cluster(c, p->rmsd_limit);
+        Env env = make_env(c, p->mode);
+        // refinement of every leader: items = (lig, chain) for all leader slots; empty slots
+        // (leader == -1) are skipped by passing only the maximal list and letting the kernel
+        // read counts on the host after a sync of the small count array.
+        std::vector<int> counts(nlig);
+        ck(cudaMemcpyAsync(counts.data(), c->d_counts.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        std::vector<int> leaders((size_t)nlig * p->nchain);
+        ck(cudaMemcpyAsync(leaders.data(), c->d_leaders.p, leaders.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                           c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "search+cluster");
+        if (p->refine_steps > 0) {
+            std::vector<int> il;
+            std::vector<long long> io;
+            int wsm = 0;
+            for (int l = 0; l < nlig; l++) {
+                const LigHost& h = c->h_ligs[l];
+                wsm = std::max(wsm, ws_floats(h.natom, h.ntors));
+                for (int k = 0; k < counts[l]; k++) {
+                    il.push_back(l);
+                    io.push_back(c->h_ligdev[l].best_off + (long long)leaders[(size_t)l * p->nchain + k] * h.stride);
+                }
+            }
+            int n = (int)il.size();
+            if (n > 0) {
+                c->d_item_lig.upload(il.data(), n, c->stream);
+                c->d_item_off.upload(io.data(), n, c->stream);
+                int W = pick_warps(c, wsm, 0, 8);
+                size_t smem = (size_t)W * wsm * 4;
+                set_smem(k_bfgs, smem);
+                k_bfgs<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, c->d_item_lig.p,
+                                                                     c->d_item_off.p, c->d_best.p, env, 2,
+                                                                     p->refine_steps, VCAP_AUTH, 100.f, 1, wsm,
+                                                                     nullptr);
+                ck(cudaGetLastError(), "k_bfgs launch");
+            }
+        }
+        // filter and gather
+        c->num_pose = p->num_pose;
+        long long of = 0;
+        for (int l = 0; l < nlig; l++) {
+            c->h_ligdev[l].out_off = of;
+            of += (long long)p->num_pose * c->h_ligs[l].stride;
+        }
+        c->out_floats = of;
+        upload_ligdev(c);
+        c->d_sel.ensure((size_t)nlig * p->num_pose);
+        c->d_selcnt.ensure(nlig);
+        c->d_out.ensure((size_t)of);
+        size_t fsm = (size_t)p->nchain * 8;
+        set_smem(k_filter, fsm);
+        k_filter<<<nlig, 128, fsm, c->stream>>>(c->d_ligs.p, nlig, p->nchain, c->d_best.p, c->d_leaders.p,
+                                                c->d_counts.p, p->num_pose, p->energy_range, c->d_sel.p, c->d_selcnt.p);
+        ck(cudaGetLastError(), "k_filter launch");
+        long long items = (long long)nlig * p->num_pose;
+        k_gather<<<(unsigned)((items + 7) / 8), 256, 0, c->stream>>>(c->d_ligs.p, nlig, p->num_pose, c->d_best.p,
+                                                                    c->d_sel.p, c->d_selcnt.p, c->d_out.p);
+        ck(cudaGetLastError(), "k_gather launch");
+        c->h_counts.assign(nlig, 0);
+        ck(cudaMemcpyAsync(c->h_counts.data(), c->d_selcnt.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+           "D2H");
+        unsigned long long ne = 0;
+        ck(cudaMemcpyAsync(&ne, c->d_nevals.p, sizeof(ne), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "refine+filter");
+        // final scoring of the selected poses (score.cpp semantics)
+        std::vector<int> pl;
+        std::vector<long long> xo, dof;
+        long long ds = 0;
+        for (int l = 0; l < nlig; l++)
+            for (int k = 0; k < c->h_counts[l]; k++) {
+                pl.push_back(l);
+                xo.push_back(c->h_ligdev[l].out_off + (long long)k * c->h_ligs[l].stride + 8);
+                dof.push_back(ds);
+                ds += 5LL * c->h_ligs[l].natom;
+            }
+        int n = (int)pl.size();
+        c->decomp = p->energy_decomp != 0;
+        if (n > 0) {
+            Env fenv = make_env(c, p->final_mode);
+            c->d_item_lig.upload(pl.data(), n, c->stream);
+            c->d_item_off.upload(xo.data(), n, c->stream);
+            c->d_item_off2.upload(dof.data(), n, c->stream);
+            c->d_terms.ensure(4 * (size_t)n);
+            if (c->decomp) c->d_decomp.ensure((size_t)ds);
+            k_terms<<<(n + 7) / 8, 256, 0, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, c->d_item_lig.p, c->d_item_off.p,
+                                                        c->d_out.p, fenv, c->d_terms.p,
+                                                        c->decomp ? c->d_decomp.p : nullptr, c->d_item_off2.p);
+            ck(cudaGetLastError(), "k_terms launch");
+            ck(cudaStreamSynchronize(c->stream), "k_terms");
+        }
+        if (out_nevals) *out_nevals = (long long)ne;
+        c->has_results = true;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_result_counts(const ud_ctx* c, int* out) {
+    if (!c || !c->has_results || !out) { g_err = "no docking results"; return UD_ESTATE; }
+    memcpy(out, c->h_counts.data(), c->h_counts.size() * sizeof(int));
+    return UD_OK;
+}
+
+long long ud_result_floats(const ud_ctx* c) {
+    if (!c || !c->has_results) return 0;
+    long long s = 0;
+    for (size_t l = 0; l < c->h_ligs.size(); l++) s += (long long)c->h_counts[l] * c->h_ligs[l].stride;
+    return s;
+}
+
+int ud_get_results(const ud_ctx* c, float* out_records, float* out_terms4, float* out_decomp) {
+    try {
+        if (!c || !c->has_results) throw Fail(UD_ESTATE, "no docking results");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        int nlig = (int)c->h_ligs.size();
+        std::vector<float> all((size_t)c->out_floats);
+        ck(cudaMemcpy(all.data(), c->d_out.p, all.size() * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
+        long long w = 0;
+        int npose = 0;
+        long long ndec = 0;
+        for (int l = 0; l < nlig; l++) {
+            long long nf = (long long)c->h_counts[l] * c->h_ligs[l].stride;
+            if (out_records) memcpy(out_records + w, all.data() + c->h_ligdev[l].out_off, nf * sizeof(float));
+            w += nf;
+            npose += c->h_counts[l];
+            ndec += 5LL * c->h_ligs[l].natom * c->h_counts[l];
+        }
+        if (out_terms4 && npose)
+            ck(cudaMemcpy(out_terms4, c->d_terms.p, 4 * (size_t)npose * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
+        if (out_decomp && c->decomp && ndec)
+            ck(cudaMemcpy(out_decomp, c->d_decomp.p, ndec * sizeof(float), cudaMemcpyDeviceToHost), "D2H");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_sync(ud_ctx* c) {
+    try {
+        if (!c) throw Fail(UD_EINVAL, "null context");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        ck(cudaStreamSynchronize(c->stream), "sync");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+}  // extern "C"

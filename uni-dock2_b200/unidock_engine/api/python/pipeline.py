@@ -1,0 +1,265 @@
+"""Drop-in replacement for the reference's pybind module ``unidock_engine.api.python.pipeline``.
+
+Same class, keyword-only constructor arguments and defaults, methods and output files as
+the reference (unidock/unidock_engine/api/python/pipeline.cpp:56-217, defaults
+src/screening/core.h:9-92 and src/model/model.h:151-167).  ``run()`` drives the B200
+engine (libudock_b200.so) instead of the reference's CUDA engine:
+
+* presets: search_mode fast/balance/detail/free (src/screening/core.cpp:65-84), task
+  screen/score/mc/randomize/optimize (core.cpp:165-212), bias no/pos/align (core.cpp:86-97),
+  constraint docking disables randomisation (core.cpp:142-146);
+* ligands are processed in the reference's size groups and batches of at most 1000
+  (src/screening/screening.cpp:17-41,162-216), one output file per batch
+  ``<output_dir>/<name_json>_<batch>.json``; ``opt_steps=-1`` resolves to
+  ``(25 + max atoms of the first batch) / 3`` and keeps that value (screening.cpp:206-208);
+* output JSON ``{ligand: [{"energy": [affinity, total, intra, inter, penalty, conf_indep,
+  bias], "coords": [...], "dihedrals": [deg...], ("decomp": [[5]...])}]}``, 3 decimals,
+  non-finite values clamped to +-1e6 (src/format/json.cpp:88-191, src/task/DockTask.cpp:224-282);
+* failures raise ``RuntimeError("Core pipeline failed...")`` (pipeline.cpp:141-143).
+
+Additional optional keyword arguments (not in the reference): ``scoring`` ("grid" or
+"direct" intermolecular term during search), ``grid_precision`` ("f32" or "f16"),
+``grid_spacing`` (A).
+"""
+from __future__ import annotations
+
+import json
+import logging
+import math
+import os
+import time
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from ud2b200.engine import Engine, EngineError, MODE_DIRECT, MODE_GRID, GRID_F16, GRID_F32, split_record
+from ud2b200.model import Box, F32, RAD2DEG_F, parse_ligands, parse_receptor
+
+log = logging.getLogger("unidock_engine")
+
+# src/screening/screening.h:19-30
+GROUP_LIMITS = [(40, 8), (80, 16), (120, 24), (160, 32)]
+BATCH_MAX = 1000
+W_CONF = F32(0.05846)
+MAX_SAFE = 1e6
+
+
+def _safe(v: float) -> float:
+    """json.cpp:78-85"""
+    if not math.isfinite(v):
+        return MAX_SAFE
+    return max(-MAX_SAFE, min(MAX_SAFE, v))
+
+
+def _fmt(v: float) -> str:
+    """Shortest float text truncated to 3 decimals (rapidjson SetMaxDecimalPlaces(3))."""
+    v = _safe(float(np.float32(v)))
+    s = repr(float(np.float32(v)))
+    if "e" in s or "E" in s:
+        s = f"{v:.6f}"
+    if "." in s:
+        ip, fp = s.split(".", 1)
+        fp = fp[:3]
+        s = ip + "." + (fp if fp else "0")
+    else:
+        s = s + ".0"
+    return s
+
+
+def _json_list(vals) -> str:
+    return "[" + ",".join(_fmt(x) for x in vals) + "]"
+
+
+class DockingPipeline:
+    """Uni-Dock2 molecular docking pipeline (B200 engine)."""
+
+    def __init__(self, *, output_dir: str = "./res_ud2", center_x: float, center_y: float, center_z: float,
+                 size_x: float, size_y: float, size_z: float, task: str = "screen", search_mode: str = "balance",
+                 exhaustiveness: int = 512, randomize: bool = True, mc_steps: int = 20, opt_steps: int = -1,
+                 refine_steps: int = 5, num_pose: int = 10, rmsd_limit: float = 1.0, energy_range: float = 10.0,
+                 seed: int = 12345, bias: str = "no", bias_k: float = 0.1, constraint_docking: bool = False,
+                 use_tor_lib: bool = False, energy_decomp: bool = False, gpu_device_id: int = 0,
+                 name_json: str = "from_python_obj", max_gpu_mem: int = 0,
+                 scoring: str = "grid", grid_precision: str = "f32", grid_spacing: float = 0.375):
+        self.output_dir = output_dir
+        self.box = Box.from_center_size([center_x, center_y, center_z], [size_x, size_y, size_z])
+        self.task = task
+        self.search_mode = search_mode
+        self.exhaustiveness = int(exhaustiveness)
+        self.randomize = bool(randomize)
+        self.mc_steps = int(mc_steps)
+        self.opt_steps = int(opt_steps)
+        self.refine_steps = int(refine_steps)
+        self.num_pose = int(num_pose)
+        self.rmsd_limit = float(rmsd_limit)
+        self.energy_range = float(energy_range)
+        self.seed = int(seed)
+        self.bias = bias
+        self.bias_k = float(bias_k)
+        self.constraint_docking = bool(constraint_docking)
+        self.use_tor_lib = bool(use_tor_lib)
+        self.energy_decomp = bool(energy_decomp)
+        self.gpu_device_id = int(gpu_device_id)
+        self.name_json = name_json
+        self.max_gpu_mem = int(max_gpu_mem)
+        self.scoring = scoring
+        self.grid_precision = grid_precision
+        self.grid_spacing = float(grid_spacing)
+        self._receptor: List = []
+        self._ligands: Dict[str, dict] = {}
+        self.last_stats: Dict[str, float] = {}
+
+    def set_receptor(self, receptor_info: list) -> None:
+        """Receptor atoms: rows [x, y, z, vina_type, ff_type, charge]."""
+        self._receptor = receptor_info
+
+    def add_ligands(self, ligands_info: dict) -> None:
+        """Ligand topologies keyed by name (later keys overwrite earlier ones)."""
+        for k, v in ligands_info.items():
+            self._ligands[k] = v
+
+    # ------------------------------------------------------------------ run
+    def _params(self) -> dict:
+        p = dict(seed=self.seed, exhaustiveness=self.exhaustiveness, randomize=self.randomize,
+                 mc_steps=self.mc_steps, opt_steps=-1 if self.opt_steps < 0 else self.opt_steps,
+                 refine_steps=self.refine_steps, num_pose=self.num_pose, energy_range=self.energy_range,
+                 rmsd_limit=self.rmsd_limit)
+        if self.bias not in ("no", "pos", "align"):
+            raise ValueError(f"Not supported bias: {self.bias} doesn't belong to (no, pos, align)")
+        p["bias_type"] = {"no": 0, "pos": 1, "align": 2}[self.bias]
+        sm = self.search_mode
+        if sm in ("", "free"):
+            pass
+        elif sm == "fast":
+            p.update(exhaustiveness=128, mc_steps=20, opt_steps=-1)
+        elif sm == "balance":
+            p.update(exhaustiveness=256, mc_steps=30, opt_steps=-1)
+        elif sm == "detail":
+            p.update(exhaustiveness=512, mc_steps=40, opt_steps=-1)
+        else:
+            raise ValueError(f"Not supported search_mode: {sm} doesn't belong to (fast, balance, detail, free)")
+        if self.constraint_docking:
+            p["randomize"] = False
+        t = self.task
+        if t == "screen":
+            pass
+        elif t == "score":
+            p.update(randomize=False, exhaustiveness=1, mc_steps=0, opt_steps=0, refine_steps=0, num_pose=1,
+                     energy_range=999.0, rmsd_limit=999.0)
+        elif t == "benchmark_one":
+            p["skip"] = True
+        elif t == "mc":
+            p.update(randomize=True, opt_steps=0, refine_steps=0)
+        elif t == "randomize":
+            p.update(randomize=True, mc_steps=0, opt_steps=0, refine_steps=0, num_pose=p["exhaustiveness"],
+                     energy_range=1e9, rmsd_limit=0.0)
+        elif t == "optimize":
+            p.update(randomize=False, exhaustiveness=1, mc_steps=0, opt_steps=0, num_pose=1, energy_range=1e9,
+                     rmsd_limit=0.0)
+        else:
+            raise ValueError(f"Not supported task: {t} doesn't belong to (screen, local_only, mc)")
+        return p
+
+    def run(self) -> None:
+        """Dock every ligand; writes <output_dir>/<name_json>_<batch>.json files."""
+        try:
+            self._run()
+        except Exception as e:  # the reference surfaces any failure as this RuntimeError
+            log.error("Core pipeline failed: %s", e)
+            raise RuntimeError(f"Core pipeline failed. {e}") from e
+
+    def _run(self) -> None:
+        t0 = time.perf_counter()
+        p = self._params()
+        os.makedirs(self.output_dir, exist_ok=True)
+        if p.get("skip"):
+            log.warning("benchmark task is not implemented")
+            return
+        rec = parse_receptor(self._receptor, self.box)
+        ligs = parse_ligands(self._ligands, self.use_tor_lib)
+        if not ligs:
+            log.error("No flexible molecules are found")
+        groups: List[List[int]] = [[] for _ in range(len(GROUP_LIMITS) + 1)]
+        for i, l in enumerate(ligs):
+            for gi, (na, nt) in enumerate(GROUP_LIMITS):
+                if l.natom <= na and l.ntors <= nt:
+                    groups[gi].append(i)
+                    break
+            else:
+                groups[-1].append(i)
+        eng = Engine(self.box, device=self.gpu_device_id)
+        try:
+            eng.set_flags(self.constraint_docking, p["bias_type"], p["bias_k"] if "bias_k" in p else self.bias_k)
+            eng.set_receptor(rec.xyz, rec.types)
+            mode = MODE_GRID if self.scoring == "grid" else MODE_DIRECT
+            if mode == MODE_GRID:
+                mt = sorted(set(int(t) for l in ligs for t in l.types if t != 0))
+                if mt:
+                    eng.build_grid(self.grid_spacing, mt, GRID_F16 if self.grid_precision == "f16" else GRID_F32)
+                else:
+                    mode = MODE_DIRECT
+            opt_steps = p["opt_steps"]
+            batch_id = 0
+            nevals = 0
+            for g in groups:
+                done = 0
+                while done < len(g):
+                    batch = g[done:done + BATCH_MAX]
+                    done += len(batch)
+                    batch_id += 1
+                    bl = [ligs[i] for i in batch]
+                    if opt_steps == -1:
+                        opt_steps = (25 + max(l.natom for l in bl)) // 3
+                    eng.clear_ligands()
+                    eng.add_ligands(bl)
+                    res, ne = eng.dock(seed=p["seed"], nchain=p["exhaustiveness"], mc_steps=p["mc_steps"],
+                                       opt_steps=opt_steps, refine_steps=p["refine_steps"], num_pose=p["num_pose"],
+                                       rmsd_limit=p["rmsd_limit"], energy_range=p["energy_range"],
+                                       randomize=p["randomize"], mode=mode, final_mode=MODE_DIRECT,
+                                       energy_decomp=self.energy_decomp)
+                    nevals += ne
+                    fp = os.path.join(self.output_dir, f"{self.name_json}_{batch_id}.json")
+                    self._dump(fp, bl, res)
+        finally:
+            eng.close()
+        self.last_stats = dict(seconds=time.perf_counter() - t0, evaluations=float(nevals), ligands=float(len(ligs)))
+
+    # ------------------------------------------------------------------ output
+    def _dump(self, fp: str, ligs, results) -> None:
+        parts = []
+        for lig, r in zip(ligs, results):
+            poses = []
+            intra_r1 = F32(r.terms[0, 0]) if len(r.records) else F32(0)
+            for k, rec in enumerate(r.records):
+                pose = split_record(lig, rec)
+                intra, inter, pen, bias = (F32(v) for v in r.terms[k])
+                total = F32(F32(intra + inter) + pen)
+                e_inter = F32(total - intra_r1)
+                aff = F32(e_inter / F32(F32(1) + W_CONF * F32(lig.ntors)))
+                conf = F32(aff - e_inter)
+                energy = [aff, total, intra, inter, pen, conf, bias]
+                dih = [F32(d * RAD2DEG_F) for d in pose["dihedrals"]]
+                s = '{"energy":' + _json_list(energy) + ',"coords":' + _json_list(pose["coords"].reshape(-1)) + \
+                    ',"dihedrals":' + _json_list(dih)
+                if self.energy_decomp and r.decomp is not None:
+                    s += ',"decomp":[' + ",".join(_json_list(a) for a in r.decomp[k]) + "]"
+                poses.append(s + "}")
+            parts.append(json.dumps(lig.name) + ":[" + ",".join(poses) + "]")
+        text = "{" + ",".join(parts) + "}"
+        wait = 5
+        for attempt in range(5):     # DockTask.cpp:285-333: retry with back-off, check completeness
+            try:
+                with open(fp, "w") as f:
+                    f.write(text)
+                    f.flush()
+                    os.fsync(f.fileno())
+                with open(fp, "rb") as f:
+                    f.seek(-1, os.SEEK_END)
+                    if f.read(1) != b"}":
+                        raise IOError("JSON file is incomplete.")
+                return
+            except Exception:
+                if attempt == 4:
+                    raise
+                time.sleep(wait)
+                wait *= 2
