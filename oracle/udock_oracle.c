@@ -378,10 +378,11 @@ R orc_grid_interp(const orc_env* env, int map, const R* x, R* g) {
     for (int a = 0; a < 3; a++) {
         R u = (x[a] - env->origin[a]) / env->spacing;
         clamped[a] = 0;
-        if (u < 0) { u = 0; clamped[a] = 1; }
+        if (!(u >= 0)) { u = 0; clamped[a] = 1; }   /* also catches NaN */
         if (u > (R)(gd[a] - 1)) { u = (R)(gd[a] - 1); clamped[a] = 1; }
         int i = (int)floor(u);
         if (i > gd[a] - 2) i = gd[a] - 2;
+        if (i < 0) i = 0;
         i0[a] = i;
         fr[a] = u - (R)i;
     }

@@ -302,11 +302,12 @@ __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x
     for (int a = 0; a < 3; a++) {
         float v = u[a];
         cl[a] = false;
-        if (v < 0.f) { v = 0.f; cl[a] = true; }
+        if (!(v >= 0.f)) { v = 0.f; cl[a] = true; }      // also catches NaN
         float hi = (float)(dim[a] - 1);
         if (v > hi) { v = hi; cl[a] = true; }
         int i = (int)floorf(v);
         if (i > dim[a] - 2) i = dim[a] - 2;
+        if (i < 0) i = 0;
         i0[a] = i;
         fr[a] = v - (float)i;
     }
