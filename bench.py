@@ -1,0 +1,324 @@
+"""Throughput benchmark of the docking engine: ligands/s on the plain virtual-screen workload.
+
+Workload ("screen"): a 4000-atom synthetic receptor, ligands with 12-48 heavy atoms and
+Poisson(5) rotatable bonds (clipped 0-12), a 30 A box with 0.375 A grid maps (81^3 x types),
+128 MC chains x 4000 steps per ligand with BFGS (opt_steps resolved by the -1 heuristic),
+5 refinement rounds of the cluster leaders, top-9 poses at RMSD 1.0 A, final scoring.
+A step docks one batch of ligands completely.  Inputs are seeded synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU, each rank docking its own ligands (weak
+scaling, no data-path collective); the timed region is bracketed by a barrier and
+synchronisation and its time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "uni-dock2_b200"))
+
+METRIC = "ligands/s @ best-score within 0.3 kcal/mol of ref; learned vs plain search"
+UNIT = "ligands/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="screen")
+    ap.add_argument("--ligands", type=int, default=0, help="ligands per step per GPU (0 = auto)")
+    ap.add_argument("--mc-steps", type=int, default=0, help="override MC steps (0 = workload value)")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--grid", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------- workload
+def make_inputs(workload: str, nlig: int, seed: int, rank: int):
+    import numpy as np
+    from ud2b200 import synth
+    from ud2b200.model import Box, parse_ligands, parse_receptor
+    w = synth.WORKLOADS[workload]
+    rows, center = synth.make_receptor(w["nrec"], w["cube"], seed)
+    box = Box.from_center_size(center, [w["box"]] * 3)
+    rec = parse_receptor(rows, box)
+    sizes = synth.ligand_sizes(workload, nlig * (rank + 1), seed)[nlig * rank:]
+    core = synth.make_core(center, seed) if workload == "template" else None
+    ligd = {f"r{rank}_lig{i:05d}": synth.make_ligand(n, t, seed * 7919 + rank * 1000003 + i, center, core=core)
+            for i, (n, t) in enumerate(sizes)}
+    ligs = parse_ligands(ligd)
+    return w, box, rec, ligs
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per heavy-atom evaluation of k_search from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_search_screen.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_heavy_atom_eval:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 4 + k and r[4 + k].lower().startswith("active"):
+                    reasons.add(n)
+        loaded = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------------- CPU port
+def cpu_port_rate(w, box, rec, ligs, mc_steps, opt_steps, seconds: float, mode: str = "direct"):
+    """Chain-steps per second of the oracle's restatement of the reference search on all
+    host cores (one chain per thread; the C calls release the GIL)."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    orc = O.Oracle("f32")
+    env = orc.make_env(rec, box, mode=mode)
+    cores = os.cpu_count() or 1
+    sample = ligs[:cores]
+    oligs = [orc.ligand(l) for l in sample]
+    done_steps = 0
+    t0 = time.perf_counter()
+    steps = 1
+    while True:
+        def run(k):
+            l = sample[k % len(sample)]
+            pose = O.initial_pose(l)
+            orc.mc_chain(oligs[k % len(sample)], env, pose, seed=11, lig_uid=k, chain=k, nchain=w["chains"],
+                         mc_steps=steps, opt_steps=opt_steps, randomize=True)
+            return steps
+        ts = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=cores) as ex:
+            done_steps += sum(ex.map(run, range(cores)))
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= mc_steps:
+            break
+        left = seconds - el
+        per = (time.perf_counter() - ts) / steps
+        steps = max(1, min(mc_steps, int(left / max(per, 1e-6))))
+    el = time.perf_counter() - t0
+    rate = done_steps / el
+    return rate, cores, f"{done_steps} MC steps of {cores} chains (one per core) on {len(sample)} screen ligands, " \
+                        f"{mode} scoring, in {el:.1f} s"
+
+
+# ------------------------------------------------------------------------- main arms
+def run_reference(a):
+    """The reference's CPU path on this host: the oracle restatement of the reference's
+    search (direct-sum scoring as the reference), timed on bounded samples."""
+    import numpy as np
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from ud2b200.batching import heuristic_opt_steps
+    nl = max(8, os.cpu_count() or 8)
+    w, box, rec, ligs = make_inputs(a.workload, nl, a.seed, 0)
+    mc = a.mc_steps or w["mc_steps"]
+    opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
+    per_step = max(2.0, min(30.0, 120.0 / max(1, a.steps + a.warmup)))
+    rates = []
+    for s in range(a.warmup + a.steps):
+        r, cores, sample = cpu_port_rate(w, box, rec, ligs, mc, opt, per_step)
+        if s >= a.warmup:
+            rates.append(r)
+    rate = statistics.mean(rates)
+    lig_s = rate / (w["chains"] * mc)
+    out = {"metric": METRIC, "value": lig_s, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": 1000.0 / lig_s, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": {"workload": a.workload, "chains": w["chains"], "mc_steps": mc, "opt_steps": opt,
+                      "receptor_atoms": rec.natom, "box_A": w["box"]},
+           "cpu_baseline": {"value": lig_s, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": lig_s, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    from ud2b200 import Engine, GRID_F16, GRID_F32, MODE_GRID
+    from ud2b200.batching import heuristic_opt_steps
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    nl = a.ligands or 296
+    w, box, rec, ligs = make_inputs(a.workload, nl, a.seed, rank)
+    mc = a.mc_steps or w["mc_steps"]
+    opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
+    eng = Engine(box, device=local)
+    eng.set_receptor(rec.xyz, rec.types)
+    mt = sorted(set(int(t) for l in ligs for t in l.types if t != 0))
+    eng.build_grid(0.375, mt, GRID_F16 if a.grid == "f16" else GRID_F32)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
+    dock_kw = dict(seed=a.seed, nchain=w["chains"], mc_steps=mc, opt_steps=opt, refine_steps=5,
+                   num_pose=w["num_pose"], rmsd_limit=w["rmsd"], energy_range=10.0, randomize=True, mode=MODE_GRID)
+    from ud2b200.engine import pack_ligands
+    packed = pack_ligands(ligs)
+    h2d = int(sum(v.nbytes for v in packed.values()))
+    dev_ms, e2e_s, stage, heavy, evals, launches = [], [], [], 0, 0, 0
+    sampler = ClockSampler(local)
+    for s in range(a.warmup + a.steps):
+        if s == a.warmup:
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            sampler.__enter__()
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.clear_ligands()
+        eng.add_ligands(ligs)
+        res, ne = eng.dock(**dock_kw, fetch=True)
+        t1 = time.perf_counter()
+        st = eng.stage_times()
+        cn = eng.counters()
+        if s >= a.warmup:
+            dev_ms.append(float(st[5]))
+            e2e_s.append(t1 - t0)
+            stage.append(st.tolist())
+            heavy += cn["heavy_atom_evaluations"]
+            evals += cn["evaluations"]
+            launches += cn["launches"]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler.__exit__()
+    d2h = int(sum(4 * (len(r.records) * (8 + 3 * l.natom + l.ntors) + 4 * len(r.records)) for r, l in zip(res, ligs)))
+    tot_ms = sum(dev_ms)
+    tot_e2e = sum(e2e_s)
+    search_ms = sum(x[0] for x in stage)
+    ligs_done = len(ligs) * a.steps
+    if dist:
+        t = torch.tensor([tot_ms, tot_e2e], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot_ms, tot_e2e = float(t[0]), float(t[1])
+        n = torch.tensor([ligs_done], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(n)
+        ligs_done = int(n.item())
+    value = ligs_done / (tot_ms / 1000.0)
+    peak, peak_kind = load_peaks()
+    bytes_alg = heavy * 8 * (2 if a.grid == "f16" else 4)
+    achieved = bytes_alg / (search_ms / 1000.0) / 1e9 if search_ms > 0 else 0.0
+    tr = load_traffic()
+    traffic = tr * heavy / a.steps if tr is not None else None
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+           "ms_per_step": tot_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f32", "data": "synthetic",
+           "config": {"workload": a.workload, "ligands_per_step_per_gpu": len(ligs), "chains": w["chains"],
+                      "mc_steps": mc, "opt_steps": opt, "refine_steps": 5, "num_pose": w["num_pose"],
+                      "rmsd_limit": w["rmsd"], "receptor_atoms": rec.natom, "box_A": w["box"], "grid_spacing_A": 0.375,
+                      "grid_maps": len(mt), "grid_precision": a.grid, "l2": "flushed between steps (256 MB write)",
+                      "parallelism": f"ligand shards x{world}"},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": traffic, "kernel": "k_search",
+                        "peak_kind": f"{peak_kind} hbm copy bandwidth",
+                        "algorithmic_bytes_per_launch": bytes_alg / a.steps},
+           "e2e": {"value": ligs_done / tot_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+           "gpu_launches": launches,
+           "stage_ms_per_step": [sum(x[i] for x in stage) / a.steps for i in range(6)],
+           "evaluations_per_step": evals / a.steps,
+           "poses_scored_per_s": evals / (search_ms / 1000.0) if search_ms > 0 else None,
+           "clocks": sampler.summary()}
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        rate, cores, sample = cpu_port_rate(w, box, rec, ligs, mc, opt, a.cpu_seconds)
+        out["cpu_baseline"] = {"value": rate / (w["chains"] * mc), "unit": UNIT, "cores": cores, "kind": "port",
+                               "sample": sample}
+    eng.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -179,6 +179,21 @@ long long ud_result_floats(const ud_ctx* ctx);
 /* Synchronise the context's stream; returns an error if a kernel failed. */
 int ud_sync(ud_ctx* ctx);
 
+/* The cudaStream_t the context launches on (for callers that time with CUDA events).
+ * No reference counterpart (the reference uses the legacy default stream). */
+void* ud_stream(ud_ctx* ctx);
+
+/* Device times (ms, CUDA events on the context's stream) of the stages of the last
+ * ud_dock: out6 = [search, cluster, refine, filter+gather, final score, total].
+ * No reference counterpart (the reference logs host wall time, screening.cpp:204-214). */
+int ud_stage_times(const ud_ctx* ctx, float* out6);
+
+/* Work counters of the last ud_search / ud_dock: out4 = [energy evaluations in the search,
+ * heavy-atom evaluations in the search (sum over evaluations of heavy atoms),
+ * kernel launches, chains].  Replaces the reference's managed line-search counter
+ * (src/cuda/common.cu:6, src/cuda/mc.cu:443). */
+int ud_counters(const ud_ctx* ctx, long long* out4);
+
 #ifdef __cplusplus
 }
 #endif

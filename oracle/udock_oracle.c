@@ -338,6 +338,15 @@ static void rng4(const orc_search_param* sp, int chain, uint32_t step, uint32_t 
     orc_philox4x32_10(ctr, key, out);
 }
 
+/* Squared distance for the 8 A cutoff test (r^2 < 64, vina.h:206), computed in double
+   with separately rounded operations.  For float-valued inputs it is exact up to the
+   final additions and identical to the engine's, so both take the same side of the
+   discontinuous cutoff. */
+static double cut_r2(double ax, double ay, double az, double bx, double by, double bz) {
+    double dx = ax - bx, dy = ay - by, dz = az - bz;
+    return (dx * dx + dy * dy) + dz * dz;
+}
+
 /* ---------------- grid model (no reference counterpart) ---------------- */
 /* map value for probe type t at point p = the reference inter pair sum for one atom of
    type t at p, without curl: sum_j eval_ef(|p-r_j| - (R_t+R_j)), |p-r_j|^2 < 64
@@ -350,16 +359,17 @@ void orc_grid_build(int nrec, const R* rx, const int* rt, int nmaps, const int* 
         int ix = (int)(idx % gd[0]);
         int iy = (int)((idx / gd[0]) % gd[1]);
         int iz = (int)(idx / ((size_t)gd[0] * gd[1]));
-        R p[3] = {origin[0] + ix * spacing, origin[1] + iy * spacing, origin[2] + iz * spacing};
+        /* grid points are float (one rounded fma), as the engine lays them out */
+        float p[3] = {fmaf((float)ix, (float)spacing, (float)origin[0]), fmaf((float)iy, (float)spacing, (float)origin[1]),
+                      fmaf((float)iz, (float)spacing, (float)origin[2])};
         for (int m = 0; m < nmaps; m++) {
             int t = map_types[m];
             R acc = 0, f;
             for (int j = 0; j < nrec; j++) {
                 if (rt[j] == VN_H) continue;
-                R d0 = rx[3 * j] - p[0], d1 = rx[3 * j + 1] - p[1], d2 = rx[3 * j + 2] - p[2];
-                R rr = d0 * d0 + d1 * d1 + d2 * d2;
+                double rr = cut_r2(rx[3 * j], rx[3 * j + 1], rx[3 * j + 2], p[0], p[1], p[2]);
                 if (rr < 64) {
-                    R r = RSQRT(rr);
+                    R r = RSQRT((R)rr);
                     acc += orc_eval_ef(r - (orc_vdw_radius(t) + orc_vdw_radius(rt[j])), t, rt[j], &f);
                 }
             }
@@ -442,9 +452,10 @@ R orc_e_f(const orc_lig* lig, const orc_env* env, const orc_pose* pose, R vcap, 
                 R rv0 = env->rec_xyz[3 * j] - X[3 * i];
                 R rv1 = env->rec_xyz[3 * j + 1] - X[3 * i + 1];
                 R rv2 = env->rec_xyz[3 * j + 2] - X[3 * i + 2];
-                R rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
+                double rr = cut_r2(env->rec_xyz[3 * j], env->rec_xyz[3 * j + 1], env->rec_xyz[3 * j + 2],
+                                   X[3 * i], X[3 * i + 1], X[3 * i + 2]);
                 if (rr < 64) {
-                    R r = RSQRT(rr);
+                    R r = RSQRT((R)rr);
                     e_atom += orc_eval_ef(r - (r1 + orc_vdw_radius(tj)), ti, tj, &fdr);
                     if (r < EPS) r = EPS;
                     fdr /= r;
@@ -591,10 +602,10 @@ void orc_score_terms(const orc_lig* lig, const orc_env* env, const R* X, R* out)
             for (int j = 0; j < env->nrec; j++) {
                 int tj = env->rec_types[j];
                 if (tj == VN_H) continue;
-                R d0 = env->rec_xyz[3 * j] - X[3 * i], d1 = env->rec_xyz[3 * j + 1] - X[3 * i + 1],
-                  d2 = env->rec_xyz[3 * j + 2] - X[3 * i + 2];
-                R rr = d0 * d0 + d1 * d1 + d2 * d2;
-                if (rr < 64) e_inter += orc_eval_ef(RSQRT(rr) - (orc_vdw_radius(ti) + orc_vdw_radius(tj)), ti, tj, &f);
+                double rr = cut_r2(env->rec_xyz[3 * j], env->rec_xyz[3 * j + 1], env->rec_xyz[3 * j + 2],
+                                   X[3 * i], X[3 * i + 1], X[3 * i + 2]);
+                if (rr < 64)
+                    e_inter += orc_eval_ef(RSQRT((R)rr) - (orc_vdw_radius(ti) + orc_vdw_radius(tj)), ti, tj, &f);
             }
         } else {
             int m = env->map_of_type[ti];

@@ -104,6 +104,17 @@ constexpr unsigned DON_MASK = (1u << 5) | (1u << 7) | (1u << 9) | (1u << 11) | (
 
 __device__ __forceinline__ float vdw(int t) { return c_vdw[t]; }
 
+// Squared distance for the 8 A cutoff test, in FP64 from float inputs with every
+// operation rounded separately: the difference of two floats and the product of two
+// such differences are exact in double, so the in/out decision at r^2 = 64 is the same
+// as the FP64 oracle's (the Vina terms are discontinuous at the cutoff).
+__device__ __forceinline__ double cutoff_r2(float ax, float ay, float az, float bx, float by, float bz) {
+    double dx = __dsub_rn((double)ax, (double)bx);
+    double dy = __dsub_rn((double)ay, (double)by);
+    double dz = __dsub_rn((double)az, (double)bz);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
 // Vina pair energy and dE/dd for surface distance d (vina.h:292-321).
 __device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
     f = 0.f;
@@ -363,10 +374,10 @@ __device__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* 
                 for (int j = 0; j < env.nrec; j++) {
                     float4 r = __ldg(env.rec + j);
                     float rv0 = r.x - px, rv1 = r.y - py, rv2 = r.z - pz;
-                    float rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
-                    if (rr < 64.f) {
+                    double rr = cutoff_r2(r.x, r.y, r.z, px, py, pz);
+                    if (rr < 64.0) {
                         int tj = (int)r.w;
-                        float rn = sqrtf(rr), fdr;
+                        float rn = sqrtf((float)rr), fdr;
                         e_atom += eval_ef(rn - (r1 + vdw(tj)), ti, tj, fdr);
                         if (rn < EPS_F) rn = EPS_F;
                         fdr /= rn;

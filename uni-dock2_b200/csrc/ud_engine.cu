@@ -94,7 +94,9 @@ __global__ void __launch_bounds__(256) k_grid_build(const float4* __restrict__ r
     long long npt = (long long)gx * gy * gz;
     long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int ix = (int)(idx % gx), iy = (int)((idx / gx) % gy), iz = (int)(idx / ((long long)gx * gy));
-    float px = ox + ix * s, py = oy + iy * s, pz = oz + iz * s;
+    // grid point in float via one rounded fma; the cutoff test below is done in FP64
+    // from the float inputs, so it is bit-identical to the oracle's
+    float px = __fmaf_rn((float)ix, s, ox), py = __fmaf_rn((float)iy, s, oy), pz = __fmaf_rn((float)iz, s, oz);
     float acc[MAX_MAPS];
     float rm[MAX_MAPS];
 #pragma unroll
@@ -107,10 +109,9 @@ __global__ void __launch_bounds__(256) k_grid_build(const float4* __restrict__ r
         if (idx < npt) {
             for (int k = 0; k < nt; k++) {
                 float4 r = tile[k];
-                float dx = r.x - px, dy = r.y - py, dz = r.z - pz;
-                float rr = dx * dx + dy * dy + dz * dz;
-                if (rr < 64.f) {
-                    float rn = sqrtf(rr);
+                double rr = cutoff_r2(r.x, r.y, r.z, px, py, pz);
+                if (rr < 64.0) {
+                    float rn = sqrtf((float)rr);
                     int tj = (int)r.w;
                     float rj = vdw(tj);
 #pragma unroll
@@ -195,11 +196,10 @@ __global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict_
         } else {
             for (int j = 0; j < env.nrec; j++) {
                 float4 r = __ldg(env.rec + j);
-                float d0 = r.x - xi, d1 = r.y - yi, d2 = r.z - zi;
-                float rr = d0 * d0 + d1 * d1 + d2 * d2;
-                if (rr < 64.f) {
+                double rr = cutoff_r2(r.x, r.y, r.z, xi, yi, zi);
+                if (rr < 64.0) {
                     int tj = (int)r.w;
-                    float d = sqrtf(rr) - (vdw(ti) + vdw(tj));
+                    float d = sqrtf((float)rr) - (vdw(ti) + vdw(tj));
                     e_inter += eval_e(d, ti, tj);
                     if (decomp) {
                         float x1 = d * 2.f, x2 = (d - 3.f) * 0.5f;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256) k_search(const int* __restrict__ blobs, c
     float* wsbase = smem + sp.blob_max;
     const int warp = threadIdx.x >> 5, lane = lane_id();
     float* ws = wsbase + (size_t)warp * sp.ws_max;
-    unsigned long long my_evals = 0;
+    unsigned long long my_evals = 0, my_heavy = 0;
     while (true) {
         if (threadIdx.x == 0) { s_lig = atomicAdd(work_counter, 1); s_next = 0; }
         __syncthreads();
@@ -382,10 +382,14 @@ __global__ void __launch_bounds__(256) k_search(const int* __restrict__ blobs, c
                 }
             }
             my_evals += ne;
+            my_heavy += (unsigned long long)ne * T.nheavy;
         }
         __syncthreads();
     }
-    if (lane == 0 && nevals) atomicAdd(nevals, my_evals);
+    if (lane == 0 && nevals) {
+        atomicAdd(nevals, my_evals);
+        atomicAdd(nevals + 1, my_heavy);
+    }
 }
 
 // ====================================================================== clustering
@@ -590,6 +594,11 @@ struct ud_ctx {
     std::vector<int> h_counts;
     bool has_results = false;
     bool decomp = false;
+    // measurement
+    cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    float stage_ms[6] = {0, 0, 0, 0, 0, 0};
+    long long counters[4] = {0, 0, 0, 0};
+    void rec(int i) { cudaEventRecord(ev[i], stream); }
 };
 
 namespace {
@@ -684,6 +693,7 @@ int ud_create(int device, const float* box6, ud_ctx** out) {
         c->device = device;
         cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
         ck(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        for (auto& e : c->ev) ck(cudaEventCreate(&e), "cudaEventCreate");
         c->box_lo[0] = box6[0]; c->box_hi[0] = box6[1];
         c->box_lo[1] = box6[2]; c->box_hi[1] = box6[3];
         c->box_lo[2] = box6[4]; c->box_hi[2] = box6[5];
@@ -705,6 +715,7 @@ int ud_destroy(ud_ctx* c) {
     c->d_sel.release(); c->d_selcnt.release(); c->d_nevals.release();
     c->d_out.release(); c->d_terms.release(); c->d_decomp.release();
     c->d_item_lig.release(); c->d_item_off.release(); c->d_item_off2.release();
+    for (auto& e : c->ev) if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return UD_OK;
@@ -1088,9 +1099,10 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     c->d_best.ensure((size_t)tot);
     c->d_order.upload(order.data(), nlig, c->stream);
     c->d_counter.ensure(1);
-    c->d_nevals.ensure(1);
+    c->d_nevals.ensure(2);
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
-    ck(cudaMemsetAsync(c->d_nevals.p, 0, sizeof(unsigned long long), c->stream), "memset");
+    ck(cudaMemsetAsync(c->d_nevals.p, 0, 2 * sizeof(unsigned long long), c->stream), "memset");
+    c->counters[3] = (long long)nlig * nchain;
     int blob_max = r4(c->max_blob);
     int W = pick_warps(c, wsm, blob_max, 8);
     size_t smem = ((size_t)blob_max + (size_t)W * wsm) * 4;
@@ -1112,7 +1124,16 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
         k_search<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_order.p, nlig, env, sp,
                                                     c->d_best.p, c->d_counter.p, c->d_nevals.p);
         ck(cudaGetLastError(), "k_search launch");
+        c->counters[2]++;
     }
+}
+
+static void read_search_counters(ud_ctx* c) {
+    unsigned long long ne[2] = {0, 0};
+    ck(cudaMemcpyAsync(ne, c->d_nevals.p, sizeof(ne), cudaMemcpyDeviceToHost, c->stream), "D2H");
+    ck(cudaStreamSynchronize(c->stream), "search counters");
+    c->counters[0] = (long long)ne[0];
+    c->counters[1] = (long long)ne[1];
 }
 
 int ud_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode,
@@ -1120,11 +1141,10 @@ int ud_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps,
     try {
         if (!c || nchain <= 0 || mc_steps < 0 || opt_steps < 0) throw Fail(UD_EINVAL, "invalid search arguments");
         ck(cudaSetDevice(c->device), "cudaSetDevice");
+        c->counters[2] = 0;
         launch_search(c, seed, nchain, mc_steps, opt_steps, randomize, mode);
-        unsigned long long ne = 0;
-        ck(cudaMemcpyAsync(&ne, c->d_nevals.p, sizeof(ne), cudaMemcpyDeviceToHost, c->stream), "D2H");
-        ck(cudaStreamSynchronize(c->stream), "k_search");
-        if (out_nevals) *out_nevals = (long long)ne;
+        read_search_counters(c);
+        if (out_nevals) *out_nevals = c->counters[0];
         c->has_results = false;
         return UD_OK;
     } catch (const Fail& f) {
@@ -1185,12 +1205,17 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
         ck(cudaSetDevice(c->device), "cudaSetDevice");
         int nlig = (int)c->h_ligs.size();
         if (nlig == 0) throw Fail(UD_ESTATE, "no ligands loaded");
+        c->counters[2] = 0;
+        sync_ligs(c);
+        c->rec(0);
         launch_search(c, p->seed, p->nchain, p->mc_steps, p->opt_steps, p->randomize, p->mode);
+        c->rec(1);
         launch_cluster(c, p->rmsd_limit);
+        c->counters[2]++;
+        c->rec(2);
         Env env = make_env(c, p->mode);
-        // refinement of every leader: items = (lig, chain) for all leader slots; empty slots
-        // (leader == -1) are skipped by passing only the maximal list and letting the kernel
-        // read counts on the host after a sync of the small count array.
+        // refinement of every cluster leader: the (ligand, chain) list is built on the host
+        // from the leader counts
         std::vector<int> counts(nlig);
         ck(cudaMemcpyAsync(counts.data(), c->d_counts.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
         std::vector<int> leaders((size_t)nlig * p->nchain);
@@ -1221,8 +1246,10 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
                                                                      p->refine_steps, VCAP_AUTH, 100.f, 1, wsm,
                                                                      nullptr);
                 ck(cudaGetLastError(), "k_bfgs launch");
+                c->counters[2]++;
             }
         }
+        c->rec(3);
         // filter and gather
         c->num_pose = p->num_pose;
         long long of = 0;
@@ -1244,12 +1271,13 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
         k_gather<<<(unsigned)((items + 7) / 8), 256, 0, c->stream>>>(c->d_ligs.p, nlig, p->num_pose, c->d_best.p,
                                                                     c->d_sel.p, c->d_selcnt.p, c->d_out.p);
         ck(cudaGetLastError(), "k_gather launch");
+        c->counters[2] += 2;
+        c->rec(4);
         c->h_counts.assign(nlig, 0);
         ck(cudaMemcpyAsync(c->h_counts.data(), c->d_selcnt.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream),
            "D2H");
-        unsigned long long ne = 0;
-        ck(cudaMemcpyAsync(&ne, c->d_nevals.p, sizeof(ne), cudaMemcpyDeviceToHost, c->stream), "D2H");
-        ck(cudaStreamSynchronize(c->stream), "refine+filter");
+        read_search_counters(c);
+        long long ne = c->counters[0];
         // final scoring of the selected poses (score.cpp semantics)
         std::vector<int> pl;
         std::vector<long long> xo, dof;
@@ -1274,9 +1302,15 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
                                                         c->d_out.p, fenv, c->d_terms.p,
                                                         c->decomp ? c->d_decomp.p : nullptr, c->d_item_off2.p);
             ck(cudaGetLastError(), "k_terms launch");
-            ck(cudaStreamSynchronize(c->stream), "k_terms");
+            c->counters[2]++;
         }
-        if (out_nevals) *out_nevals = (long long)ne;
+        c->rec(5);
+        ck(cudaStreamSynchronize(c->stream), "k_terms");
+        float t[5];
+        for (int i = 0; i < 5; i++) ck(cudaEventElapsedTime(&t[i], c->ev[i], c->ev[i + 1]), "event time");
+        for (int i = 0; i < 5; i++) c->stage_ms[i] = t[i];
+        ck(cudaEventElapsedTime(&c->stage_ms[5], c->ev[0], c->ev[5]), "event time");
+        if (out_nevals) *out_nevals = ne;
         c->has_results = true;
         return UD_OK;
     } catch (const Fail& f) {
@@ -1322,6 +1356,20 @@ int ud_get_results(const ud_ctx* c, float* out_records, float* out_terms4, float
     } catch (const Fail& f) {
         return fail(f);
     }
+}
+
+void* ud_stream(ud_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int ud_stage_times(const ud_ctx* c, float* out6) {
+    if (!c || !out6) { g_err = "null argument"; return UD_EINVAL; }
+    memcpy(out6, c->stage_ms, sizeof(c->stage_ms));
+    return UD_OK;
+}
+
+int ud_counters(const ud_ctx* c, long long* out4) {
+    if (!c || !out4) { g_err = "null argument"; return UD_EINVAL; }
+    memcpy(out4, c->counters, sizeof(c->counters));
+    return UD_OK;
 }
 
 int ud_sync(ud_ctx* c) {

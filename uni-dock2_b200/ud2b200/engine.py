@@ -71,6 +71,9 @@ def load_library() -> C.CDLL:
         "ud_get_results": ([vp, fp, fp, fp], i),
         "ud_result_floats": ([vp], C.c_longlong),
         "ud_sync": ([vp], i),
+        "ud_stream": ([vp], C.c_void_p),
+        "ud_stage_times": ([vp, fp], i),
+        "ud_counters": ([vp, ip], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -298,13 +301,30 @@ class Engine:
 
     def dock(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, refine_steps: int, num_pose: int,
              rmsd_limit: float, energy_range: float, randomize: bool = True, mode: int = MODE_GRID,
-             final_mode: int = MODE_DIRECT, energy_decomp: bool = False) -> Tuple[List[DockResult], int]:
+             final_mode: int = MODE_DIRECT, energy_decomp: bool = False,
+             fetch: bool = True) -> Tuple[Optional[List[DockResult]], int]:
         p = DockParams(seed & (2 ** 64 - 1), nchain, mc_steps, opt_steps, refine_steps, num_pose, rmsd_limit,
                        energy_range, int(randomize), mode, final_mode, int(energy_decomp))
         ne = C.c_longlong(0)
         self._check(self.L.ud_dock(self.h, C.byref(p), C.byref(ne)))
         self.nchain = nchain
-        return self.results(energy_decomp), int(ne.value)
+        return (self.results(energy_decomp) if fetch else None), int(ne.value)
+
+    @property
+    def stream_ptr(self) -> int:
+        """cudaStream_t of the context (wrap with torch.cuda.ExternalStream to time it)."""
+        return int(self.L.ud_stream(self.h) or 0)
+
+    def stage_times(self) -> np.ndarray:
+        """Device ms of the last dock: search, cluster, refine, filter, final score, total."""
+        t = np.zeros(6, np.float32)
+        self._check(self.L.ud_stage_times(self.h, _p(t)))
+        return t
+
+    def counters(self) -> dict:
+        c = np.zeros(4, np.int64)
+        self._check(self.L.ud_counters(self.h, _p(c)))
+        return dict(evaluations=int(c[0]), heavy_atom_evaluations=int(c[1]), launches=int(c[2]), chains=int(c[3]))
 
     def results(self, energy_decomp: bool = False) -> List[DockResult]:
         nl = len(self.ligands)

@@ -32,14 +32,12 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
+from ud2b200.batching import batches
 from ud2b200.engine import Engine, EngineError, MODE_DIRECT, MODE_GRID, GRID_F16, GRID_F32, split_record
 from ud2b200.model import Box, F32, RAD2DEG_F, parse_ligands, parse_receptor
 
 log = logging.getLogger("unidock_engine")
 
-# src/screening/screening.h:19-30
-GROUP_LIMITS = [(40, 8), (80, 16), (120, 24), (160, 32)]
-BATCH_MAX = 1000
 W_CONF = F32(0.05846)
 MAX_SAFE = 1e6
 
@@ -179,17 +177,10 @@ class DockingPipeline:
         ligs = parse_ligands(self._ligands, self.use_tor_lib)
         if not ligs:
             log.error("No flexible molecules are found")
-        groups: List[List[int]] = [[] for _ in range(len(GROUP_LIMITS) + 1)]
-        for i, l in enumerate(ligs):
-            for gi, (na, nt) in enumerate(GROUP_LIMITS):
-                if l.natom <= na and l.ntors <= nt:
-                    groups[gi].append(i)
-                    break
-            else:
-                groups[-1].append(i)
+        plan = batches([l.natom for l in ligs], [l.ntors for l in ligs])
         eng = Engine(self.box, device=self.gpu_device_id)
         try:
-            eng.set_flags(self.constraint_docking, p["bias_type"], p["bias_k"] if "bias_k" in p else self.bias_k)
+            eng.set_flags(self.constraint_docking, p["bias_type"], self.bias_k)
             eng.set_receptor(rec.xyz, rec.types)
             mode = MODE_GRID if self.scoring == "grid" else MODE_DIRECT
             if mode == MODE_GRID:
@@ -201,25 +192,21 @@ class DockingPipeline:
             opt_steps = p["opt_steps"]
             batch_id = 0
             nevals = 0
-            for g in groups:
-                done = 0
-                while done < len(g):
-                    batch = g[done:done + BATCH_MAX]
-                    done += len(batch)
-                    batch_id += 1
-                    bl = [ligs[i] for i in batch]
-                    if opt_steps == -1:
-                        opt_steps = (25 + max(l.natom for l in bl)) // 3
-                    eng.clear_ligands()
-                    eng.add_ligands(bl)
-                    res, ne = eng.dock(seed=p["seed"], nchain=p["exhaustiveness"], mc_steps=p["mc_steps"],
-                                       opt_steps=opt_steps, refine_steps=p["refine_steps"], num_pose=p["num_pose"],
-                                       rmsd_limit=p["rmsd_limit"], energy_range=p["energy_range"],
-                                       randomize=p["randomize"], mode=mode, final_mode=MODE_DIRECT,
-                                       energy_decomp=self.energy_decomp)
-                    nevals += ne
-                    fp = os.path.join(self.output_dir, f"{self.name_json}_{batch_id}.json")
-                    self._dump(fp, bl, res)
+            for batch in plan:
+                batch_id += 1
+                bl = [ligs[i] for i in batch]
+                if opt_steps == -1:
+                    opt_steps = (25 + max(l.natom for l in bl)) // 3
+                eng.clear_ligands()
+                eng.add_ligands(bl)
+                res, ne = eng.dock(seed=p["seed"], nchain=p["exhaustiveness"], mc_steps=p["mc_steps"],
+                                   opt_steps=opt_steps, refine_steps=p["refine_steps"], num_pose=p["num_pose"],
+                                   rmsd_limit=p["rmsd_limit"], energy_range=p["energy_range"],
+                                   randomize=p["randomize"], mode=mode, final_mode=MODE_DIRECT,
+                                   energy_decomp=self.energy_decomp)
+                nevals += ne
+                fp = os.path.join(self.output_dir, f"{self.name_json}_{batch_id}.json")
+                self._dump(fp, bl, res)
         finally:
             eng.close()
         self.last_stats = dict(seconds=time.perf_counter() - t0, evaluations=float(nevals), ligands=float(len(ligs)))
