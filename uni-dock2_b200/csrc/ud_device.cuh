@@ -3,9 +3,9 @@
 // One warp owns one pose (a Monte Carlo chain, a BFGS job or a scoring job).  The
 // ligand topology is a packed blob of 32-bit words (layout below) that kernels stage
 // in shared memory; pose state (coordinates, dihedrals, centre, last rotation
-// increment) lives in per-warp shared memory slots.  All per-atom work is strided
-// over the 32 lanes; scalar decisions are taken by lane 0 and broadcast by shuffle;
-// reductions are xor-butterflies, so results are deterministic.
+// increment) lives in per-warp shared-memory slots.  Per-atom work is strided over
+// the 32 lanes, per-torsion scalar work runs lane-parallel, reductions are fixed
+// xor-butterflies (results are deterministic run to run).
 //
 // The arithmetic follows the reference engine (paths relative to
 // unidock/unidock_engine/): Vina terms src/score/vina.h:151-321; E/force
@@ -32,45 +32,75 @@ constexpr float VCAP_AUTH = 1000.0f;
 constexpr int LS_STEPS = 10;
 
 // ---------------------------------------------------------------- blob layout
+// Header words; section offsets are word offsets from the blob start.
 enum BlobHdr {
     H_NATOM = 0, H_NTORS, H_NHEAVY, H_NPAIR, H_NROT, H_NRANGE, H_NBIAS,
-    H_TYPES, H_AXIS, H_RANGE_OFF, H_RANGES, H_ROT_OFF, H_ROT, H_PAIR_OFF, H_PAIRS,
-    H_BIAS_OFF, H_BIAS, H_HEAVY, H_X0, H_D0, H_C0, H_TOTAL, H_RES1, H_RES2,
-    H_WORDS = 24
+    H_TYPES,       // natom ints
+    H_AXIS,        // 2T ints (from, to)
+    H_RANGE_OFF,   // T+1 ints (in ranges)
+    H_RANGES,      // 2*nrange floats
+    H_ROT_OFF,     // T+1 ints
+    H_ROT,         // rotated atoms of every torsion
+    H_PAIR_OFF,    // natom+1 ints: per-atom intra adjacency (both directions)
+    H_PAIRS,       // packed entries: j | zero<<16 | hydrophobic pair<<17 | hbond pair<<18
+    H_BIAS_OFF,    // natom+1 ints (records)
+    H_BIAS,        // 5 floats per record
+    H_HEAVY,       // heavy atom indices
+    H_X0, H_D0, H_C0,   // initial coordinates, dihedrals, centre
+    H_RADII,       // natom floats: vdW radius per atom
+    H_RHOFF,       // T+1 ints: heavy rotated atoms per torsion
+    H_RHEAVY,
+    H_MAPIDX,      // natom ints: grid map slot of each atom (-1: none), set at upload
+    H_TOTAL,
+    H_WORDS = 28
 };
+constexpr int PAIR_ZERO = 1 << 16, PAIR_HYD = 1 << 17, PAIR_HB = 1 << 18;
 
+// Topology view: one base pointer and word offsets (keeps addressing 32-bit).
 struct Topo {
+    const int* b;
     int natom, ntors, nheavy, nbias;
-    const int* types;
-    const int* axis;
-    const int* range_off;
-    const float* ranges;
-    const int* rot_off;
-    const int* rot;
-    const int* pair_off;
-    const int* pairs;
-    const int* bias_off;
-    const float* bias;
-    const int* heavy;
+    int o_types, o_axis, o_roff, o_ranges, o_rot_off, o_rot, o_pair_off, o_pairs, o_bias_off, o_bias, o_heavy,
+        o_radii, o_rhoff, o_rheavy, o_mapidx;
+    __device__ __forceinline__ int type(int i) const { return b[o_types + i]; }
+    __device__ __forceinline__ int axis(int k) const { return b[o_axis + k]; }
+    __device__ __forceinline__ int range_off(int k) const { return b[o_roff + k]; }
+    __device__ __forceinline__ const float* ranges() const { return reinterpret_cast<const float*>(b + o_ranges); }
+    __device__ __forceinline__ int rot_off(int k) const { return b[o_rot_off + k]; }
+    __device__ __forceinline__ int rot(int q) const { return b[o_rot + q]; }
+    __device__ __forceinline__ int pair_off(int i) const { return b[o_pair_off + i]; }
+    __device__ __forceinline__ int pair(int k) const { return b[o_pairs + k]; }
+    __device__ __forceinline__ int bias_off(int i) const { return b[o_bias_off + i]; }
+    __device__ __forceinline__ const float* bias() const { return reinterpret_cast<const float*>(b + o_bias); }
+    __device__ __forceinline__ int heavy(int h) const { return b[o_heavy + h]; }
+    __device__ __forceinline__ float radius(int i) const { return __int_as_float(b[o_radii + i]); }
+    __device__ __forceinline__ int rh_off(int k) const { return b[o_rhoff + k]; }
+    __device__ __forceinline__ int rheavy(int q) const { return b[o_rheavy + q]; }
+    __device__ __forceinline__ int map_index(int i) const { return b[o_mapidx + i]; }
 };
 
 __device__ __forceinline__ Topo topo_view(const int* b) {
     Topo t;
+    t.b = b;
     t.natom = b[H_NATOM];
     t.ntors = b[H_NTORS];
     t.nheavy = b[H_NHEAVY];
     t.nbias = b[H_NBIAS];
-    t.types = b + b[H_TYPES];
-    t.axis = b + b[H_AXIS];
-    t.range_off = b + b[H_RANGE_OFF];
-    t.ranges = reinterpret_cast<const float*>(b + b[H_RANGES]);
-    t.rot_off = b + b[H_ROT_OFF];
-    t.rot = b + b[H_ROT];
-    t.pair_off = b + b[H_PAIR_OFF];
-    t.pairs = b + b[H_PAIRS];
-    t.bias_off = b + b[H_BIAS_OFF];
-    t.bias = reinterpret_cast<const float*>(b + b[H_BIAS]);
-    t.heavy = b + b[H_HEAVY];
+    t.o_types = b[H_TYPES];
+    t.o_axis = b[H_AXIS];
+    t.o_roff = b[H_RANGE_OFF];
+    t.o_ranges = b[H_RANGES];
+    t.o_rot_off = b[H_ROT_OFF];
+    t.o_rot = b[H_ROT];
+    t.o_pair_off = b[H_PAIR_OFF];
+    t.o_pairs = b[H_PAIRS];
+    t.o_bias_off = b[H_BIAS_OFF];
+    t.o_bias = b[H_BIAS];
+    t.o_heavy = b[H_HEAVY];
+    t.o_radii = b[H_RADII];
+    t.o_rhoff = b[H_RHOFF];
+    t.o_rheavy = b[H_RHEAVY];
+    t.o_mapidx = b[H_MAPIDX];
     return t;
 }
 
@@ -92,7 +122,6 @@ struct Env {
     const float4* rec;        // x y z type(as float)
     int nrec;
     GridView grid;
-    signed char map_of_type[NT + 3];
 };
 
 __constant__ float c_vdw[NT] = {1.1f, 1.92f, 1.9f, 1.9f, 1.8f, 1.8f, 1.8f, 1.8f, 1.7f, 1.7f, 1.7f,
@@ -103,6 +132,14 @@ constexpr unsigned ACC_MASK = (1u << 6) | (1u << 7) | (1u << 10) | (1u << 11);
 constexpr unsigned DON_MASK = (1u << 5) | (1u << 7) | (1u << 9) | (1u << 11) | (1u << 20);
 
 __device__ __forceinline__ float vdw(int t) { return c_vdw[t]; }
+
+__device__ __forceinline__ bool hyd_pair(int t1, int t2) {
+    return ((1u << t1) & HYD_MASK) && ((1u << t2) & HYD_MASK);
+}
+__device__ __forceinline__ bool hb_pair(int t1, int t2) {
+    unsigned b1 = 1u << t1, b2 = 1u << t2;
+    return ((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK));
+}
 
 // Squared distance for the 8 A cutoff test, in FP64 from float inputs with every
 // operation rounded separately: the difference of two floats and the product of two
@@ -115,10 +152,9 @@ __device__ __forceinline__ double cutoff_r2(float ax, float ay, float az, float 
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
-// Vina pair energy and dE/dd for surface distance d (vina.h:292-321).
-__device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
-    f = 0.f;
-    if (t1 == VN_H || t2 == VN_H) return 0.f;
+// Vina pair energy and dE/dd at surface distance d for a heavy pair with the given
+// pair flags (vina.h:292-321).
+__device__ __forceinline__ float vina_ef(float d, bool hyd, bool hb, float& f) {
     float x1 = d * 2.0f;                    // (d - 0) / 0.5
     float e1 = __expf(-x1 * x1);
     float x2 = (d - 3.0f) * 0.5f;           // (d - 3) / 2
@@ -129,16 +165,21 @@ __device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
         e += 0.840245f * d * d;
         f += 0.840245f * 2.f * d;
     }
-    unsigned b1 = 1u << t1, b2 = 1u << t2;
-    if ((b1 & HYD_MASK) && (b2 & HYD_MASK)) {
+    if (hyd) {
         if (d <= 0.5f) e += -0.035069f;
         else if (d < 1.5f) { e += -0.035069f * (1.5f - d); f += -0.035069f * -1.0f; }
     }
-    if (((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK))) {
+    if (hb) {
         if (d <= -0.7f) e += -0.587439f;
         else if (d < 0.f) { e += -0.587439f * (0.f - d) / 0.7f; f += -0.587439f * (1.f / -0.7f); }
     }
     return e;
+}
+
+__device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
+    f = 0.f;
+    if (t1 == VN_H || t2 == VN_H) return 0.f;
+    return vina_ef(d, hyd_pair(t1, t2), hb_pair(t1, t2), f);
 }
 
 // ---------------------------------------------------------------- warp helpers
@@ -149,10 +190,27 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
     return v;
 }
-__device__ __forceinline__ double warp_sum_d(double v) {
+
+// Reduce-scatter of 16 per-lane values: after the call, a[0] of lane L holds the warp
+// total of value v = bit4(L)<<3 | bit3(L)<<2 | bit2(L)<<1 | bit1(L).  16 shuffles
+// instead of 80 for 16 separate butterflies; the summation order is fixed.
+__device__ __forceinline__ void reduce_scatter16(float (&a)[16]) {
+    const int lane = lane_id();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
+    for (int s = 0; s < 4; s++) {
+        const int o = 16 >> s, m = 16 >> s, h = m >> 1;
+        const bool up = lane & o;
+#pragma unroll
+        for (int j = 0; j < h; j++) {
+            float send = up ? a[j] : a[j + h];
+            float keep = up ? a[j + h] : a[j];
+            a[j] = keep + __shfl_xor_sync(FULL, send, o);
+        }
+    }
+    a[0] += __shfl_xor_sync(FULL, a[0], 1);
+}
+__device__ __forceinline__ int rs16_lane(int v) {
+    return (((v >> 3) & 1) << 4) | (((v >> 2) & 1) << 3) | (((v >> 1) & 1) << 2) | ((v & 1) << 1);
 }
 
 // ---------------------------------------------------------------- RNG: Philox4x32-10
@@ -205,77 +263,84 @@ __device__ __forceinline__ float clamp_by_ranges(float a, const float* r, int n)
     }
     return best;
 }
-__device__ __forceinline__ void rotvec_to_quat(float vx, float vy, float vz, float* q) {  // quaternion.h:90-107
+__device__ __forceinline__ void rotvec_to_quat(float vx, float vy, float vz, float& q0, float& q1, float& q2,
+                                               float& q3) {  // quaternion.h:90-107
     float th = sqrtf(vx * vx + vy * vy + vz * vz);
     if (th > EPS_F) {
         float s, c;
         sincosf(th * 0.5f, &s, &c);
-        q[0] = c;
-        q[1] = s * (vx / th);
-        q[2] = s * (vy / th);
-        q[3] = s * (vz / th);
+        q0 = c;
+        q1 = s * (vx / th);
+        q2 = s * (vy / th);
+        q3 = s * (vz / th);
     } else {
-        q[0] = 1.f; q[1] = q[2] = q[3] = 0.f;
+        q0 = 1.f; q1 = q2 = q3 = 0.f;
     }
 }
 // v' = q v q* expanded (quaternion.h:185-196)
-__device__ __forceinline__ void quat_rotate(const float* q, float& x, float& y, float& z) {
-    float w0 = -q[1] * x - q[2] * y - q[3] * z;
-    float w1 = q[0] * x + q[2] * z - q[3] * y;
-    float w2 = q[0] * y - q[1] * z + q[3] * x;
-    float w3 = q[0] * z + q[1] * y - q[2] * x;
-    // (w) * conj(q)
-    float nx = -w0 * q[1] + w1 * q[0] - w2 * q[3] + w3 * q[2];
-    float ny = -w0 * q[2] + w1 * q[3] + w2 * q[0] - w3 * q[1];
-    float nz = -w0 * q[3] - w1 * q[2] + w2 * q[1] + w3 * q[0];
+__device__ __forceinline__ void quat_rotate(float q0, float q1, float q2, float q3, float& x, float& y, float& z) {
+    float w0 = -q1 * x - q2 * y - q3 * z;
+    float w1 = q0 * x + q2 * z - q3 * y;
+    float w2 = q0 * y - q1 * z + q3 * x;
+    float w3 = q0 * z + q1 * y - q2 * x;
+    float nx = -w0 * q1 + w1 * q0 - w2 * q3 + w3 * q2;
+    float ny = -w0 * q2 + w1 * q3 + w2 * q0 - w3 * q1;
+    float nz = -w0 * q3 - w1 * q2 + w2 * q1 + w3 * q0;
     x = nx; y = ny; z = nz;
 }
-__device__ __forceinline__ void quat_to_rotvec(const float* q, float* v) {  // quaternion.h:115-130
-    float th = 2.f * acosf(q[0]);
+__device__ __forceinline__ void quat_to_rotvec(float q0, float q1, float q2, float q3, float* v) {
+    float th = 2.f * acosf(q0);
     float s = sinf(th * 0.5f);
     if (s > EPS_F) {
         float k = th / s;
-        v[0] = q[1] * k; v[1] = q[2] * k; v[2] = q[3] * k;
+        v[0] = q1 * k; v[1] = q2 * k; v[2] = q3 * k;
     } else {
         v[0] = v[1] = v[2] = 0.f;
     }
 }
 
-// dR/dv_ind (rotation.h:80-144) contracted with a 3x3 matrix (row major)
-__device__ float frob_drdv(const float* mat, float vx, float vy, float vz, int ind) {
-    float v[3] = {vx, vy, vz};
+// <M, dR/dv_ind>_F with dR/dv from rotation.h:80-144 (Bailey et al. 2013), the shared
+// angle terms precomputed by the caller; M row major.
+struct RotGradBasis { float s, c, sdt, omc, vb0, vb1, vb2; };
+__device__ __forceinline__ RotGradBasis rot_grad_basis(float vx, float vy, float vz) {
+    RotGradBasis B;
     float ang = sqrtf(vx * vx + vy * vy + vz * vz);
-    float th, vb[3];
+    float th;
     if (ang > EPS_F) {
         th = normalize_angle_2pi(ang);
         if (th > PI_F) { th = 2.f * PI_F - th; ang = -ang; }
-        vb[0] = v[0] / ang; vb[1] = v[1] / ang; vb[2] = v[2] / ang;
+        B.vb0 = vx / ang; B.vb1 = vy / ang; B.vb2 = vz / ang;
     } else {
-        th = 0.f; vb[0] = vb[1] = vb[2] = 0.f;
+        th = 0.f; B.vb0 = B.vb1 = B.vb2 = 0.f;
     }
-    float s, c;
-    sincosf(th, &s, &c);
-    float e[3] = {0.f, 0.f, 0.f};
-    e[ind] = 1.f;
-    float sk[9] = {0.f, -vb[2], vb[1], vb[2], 0.f, -vb[0], -vb[1], vb[0], 0.f};
-    float a = vb[0] * vb[0], b = vb[1] * vb[1], cc = vb[2] * vb[2];
-    float sk2[9] = {-b - cc, vb[0] * vb[1], vb[0] * vb[2], vb[0] * vb[1], -a - cc, vb[1] * vb[2],
-                    vb[0] * vb[2], vb[1] * vb[2], -a - b};
-    float sdt, omc;
-    if (th > EPS_F) { sdt = s / th; omc = (1.f - c) / th; }
-    else { float t2 = th * th; sdt = 1.f - t2 / 6.f; omc = th / 2.f - th * t2 / 24.f; }
-    float vs[3] = {e[0] - vb[ind] * vb[0], e[1] - vb[ind] * vb[1], e[2] - vb[ind] * vb[2]};
-    float ts[9] = {0.f, -vs[2], vs[1], vs[2], 0.f, -vs[0], -vs[1], vs[0], 0.f};
+    sincosf(th, &B.s, &B.c);
+    if (th > EPS_F) { B.sdt = B.s / th; B.omc = (1.f - B.c) / th; }
+    else { float t2 = th * th; B.sdt = 1.f - t2 / 6.f; B.omc = th / 2.f - th * t2 / 24.f; }
+    return B;
+}
+__device__ __forceinline__ float frob_drdv(const RotGradBasis& B, int ind, float m0, float m1, float m2, float m3,
+                                           float m4, float m5, float m6, float m7, float m8) {
+    const float vb[3] = {B.vb0, B.vb1, B.vb2};
+    const float vi = ind == 0 ? B.vb0 : (ind == 1 ? B.vb1 : B.vb2);
+    const float e0 = ind == 0 ? 1.f : 0.f, e1 = ind == 1 ? 1.f : 0.f, e2 = ind == 2 ? 1.f : 0.f;
+    const float e[3] = {e0, e1, e2};
+    const float sk[9] = {0.f, -vb[2], vb[1], vb[2], 0.f, -vb[0], -vb[1], vb[0], 0.f};
+    const float a = vb[0] * vb[0], bq = vb[1] * vb[1], cq = vb[2] * vb[2];
+    const float sk2[9] = {-bq - cq, vb[0] * vb[1], vb[0] * vb[2], vb[0] * vb[1], -a - cq, vb[1] * vb[2],
+                          vb[0] * vb[2], vb[1] * vb[2], -a - bq};
+    const float vs[3] = {e0 - vi * vb[0], e1 - vi * vb[1], e2 - vi * vb[2]};
+    const float ts[9] = {0.f, -vs[2], vs[1], vs[2], 0.f, -vs[0], -vs[1], vs[0], 0.f};
+    const float m[9] = {m0, m1, m2, m3, m4, m5, m6, m7, m8};
     float acc = 0.f;
 #pragma unroll
     for (int i = 0; i < 3; i++) {
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            int k = i * 3 + j;
-            float g = c * vb[ind] * sk[k] + s * vb[ind] * sk2[k];
-            float mc = e[i] * vb[j] + vb[i] * e[j] - 2.f * vb[ind] * vb[i] * vb[j];
-            g += sdt * ts[k] + omc * mc;
-            acc += mat[k] * g;
+            const int k = i * 3 + j;
+            float g = B.c * vi * sk[k] + B.s * vi * sk2[k];
+            float mc = e[i] * vb[j] + vb[i] * e[j] - 2.f * vi * vb[i] * vb[j];
+            g += B.sdt * ts[k] + B.omc * mc;
+            acc += m[k] * g;
         }
     }
     return acc;
@@ -289,11 +354,8 @@ struct Slot {
     float* d;    // dihedrals T
 };
 __device__ __forceinline__ Slot slot_at(float* base, int stride, int idx, int natom) {
-    float* p = base + (size_t)idx * stride;
+    float* p = base + idx * stride;
     return {p, p + 8, p + 8 + 3 * natom};
-}
-__device__ __forceinline__ int slot_stride(int natom, int ntors) {
-    return (8 + 3 * natom + ntors + 3) & ~3;
 }
 __device__ __forceinline__ void slot_copy(Slot dst, Slot src, int natom, int ntors) {
     int n = 8 + 3 * natom + ntors;
@@ -304,27 +366,21 @@ __device__ __forceinline__ void slot_copy(Slot dst, Slot src, int natom, int nto
 // ---------------------------------------------------------------- grid sample
 __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x, float y, float z,
                                              float& gx_, float& gy_, float& gz_) {
-    float u[3] = {(x - g.ox) * g.inv_s, (y - g.oy) * g.inv_s, (z - g.oz) * g.inv_s};
-    int dim[3] = {g.gx, g.gy, g.gz};
-    int i0[3];
-    float fr[3];
-    bool cl[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        float v = u[a];
-        cl[a] = false;
-        if (!(v >= 0.f)) { v = 0.f; cl[a] = true; }      // also catches NaN
-        float hi = (float)(dim[a] - 1);
-        if (v > hi) { v = hi; cl[a] = true; }
-        int i = (int)floorf(v);
-        if (i > dim[a] - 2) i = dim[a] - 2;
-        if (i < 0) i = 0;
-        i0[a] = i;
-        fr[a] = v - (float)i;
-    }
-    size_t npt = (size_t)g.gx * g.gy * g.gz;
-    size_t base = (size_t)map * npt + ((size_t)i0[2] * g.gy + i0[1]) * g.gx + i0[0];
-    size_t sy = g.gx, sz = (size_t)g.gx * g.gy;
+    float u0 = (x - g.ox) * g.inv_s, u1 = (y - g.oy) * g.inv_s, u2 = (z - g.oz) * g.inv_s;
+    bool c0 = false, c1 = false, c2 = false;
+    if (!(u0 >= 0.f)) { u0 = 0.f; c0 = true; }      // also catches NaN
+    if (!(u1 >= 0.f)) { u1 = 0.f; c1 = true; }
+    if (!(u2 >= 0.f)) { u2 = 0.f; c2 = true; }
+    const float h0 = (float)(g.gx - 1), h1 = (float)(g.gy - 1), h2 = (float)(g.gz - 1);
+    if (u0 > h0) { u0 = h0; c0 = true; }
+    if (u1 > h1) { u1 = h1; c1 = true; }
+    if (u2 > h2) { u2 = h2; c2 = true; }
+    int i0 = min(max((int)floorf(u0), 0), g.gx - 2);
+    int i1 = min(max((int)floorf(u1), 0), g.gy - 2);
+    int i2 = min(max((int)floorf(u2), 0), g.gz - 2);
+    const float fx = u0 - (float)i0, fy = u1 - (float)i1, fz = u2 - (float)i2;
+    const size_t sy = g.gx, sz = (size_t)g.gx * g.gy;
+    const size_t base = (size_t)map * ((size_t)g.gz * sz) + (size_t)i2 * sz + (size_t)i1 * sy + i0;
     float v0, v1, v2, v3, v4, v5, v6, v7;
     if (g.use_f16) {
         const __half* m = g.f16 + base;
@@ -339,44 +395,44 @@ __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x
         v4 = __ldg(m + sz); v5 = __ldg(m + sz + 1);
         v6 = __ldg(m + sz + sy); v7 = __ldg(m + sz + sy + 1);
     }
-    float fx = fr[0], fy = fr[1], fz = fr[2];
-    float hx = 1.f - fx, hy = 1.f - fy, hz = 1.f - fz;
-    float c00 = v0 * hx + v1 * fx, c10 = v2 * hx + v3 * fx;
-    float c01 = v4 * hx + v5 * fx, c11 = v6 * hx + v7 * fx;
-    float c0 = c00 * hy + c10 * fy, c1 = c01 * hy + c11 * fy;
-    float e = c0 * hz + c1 * fz;
-    float ddx = ((v1 - v0) * hy + (v3 - v2) * fy) * hz + ((v5 - v4) * hy + (v7 - v6) * fy) * fz;
-    float ddy = (c10 - c00) * hz + (c11 - c01) * fz;
-    float ddz = c1 - c0;
-    gx_ = cl[0] ? 0.f : ddx * g.inv_s;
-    gy_ = cl[1] ? 0.f : ddy * g.inv_s;
-    gz_ = cl[2] ? 0.f : ddz * g.inv_s;
+    const float hx = 1.f - fx, hy = 1.f - fy, hz = 1.f - fz;
+    const float c00 = v0 * hx + v1 * fx, c10 = v2 * hx + v3 * fx;
+    const float c01 = v4 * hx + v5 * fx, c11 = v6 * hx + v7 * fx;
+    const float cc0 = c00 * hy + c10 * fy, cc1 = c01 * hy + c11 * fy;
+    const float e = cc0 * hz + cc1 * fz;
+    const float ddx = ((v1 - v0) * hy + (v3 - v2) * fy) * hz + ((v5 - v4) * hy + (v7 - v6) * fy) * fz;
+    const float ddy = (c10 - c00) * hz + (c11 - c01) * fz;
+    const float ddz = cc1 - cc0;
+    gx_ = c0 ? 0.f : ddx * g.inv_s;
+    gy_ = c1 ? 0.f : ddy * g.inv_s;
+    gz_ = c2 ? 0.f : ddz * g.inv_s;
     return e;
 }
 
 // ---------------------------------------------------------------- energy + force
 // Fills F (3N, dE/dx per atom) and returns the warp-summed energy (bfgs.cuh:221-394).
-__device__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* F, float vcap, float slope) {
+__device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* F, float vcap,
+                                          float slope) {
     const int lane = lane_id();
     float energy = 0.f;
     // inter + penalty
     for (int i = lane; i < T.natom; i += WARP) {
-        int ti = T.types[i];
+        const int ti = T.type(i);
         float fx = 0.f, fy = 0.f, fz = 0.f;
         if (ti != VN_H) {
-            float px = X[3 * i], py = X[3 * i + 1], pz = X[3 * i + 2];
+            const float px = X[3 * i], py = X[3 * i + 1], pz = X[3 * i + 2];
             float e_atom = 0.f;
             if (env.mode == 1) {
-                int m = env.map_of_type[ti];
+                const int m = T.map_index(i);
                 if (m >= 0) e_atom = grid_sample(env.grid, m, px, py, pz, fx, fy, fz);
             } else {
-                float r1 = vdw(ti);
+                const float r1 = T.radius(i);
                 for (int j = 0; j < env.nrec; j++) {
-                    float4 r = __ldg(env.rec + j);
-                    float rv0 = r.x - px, rv1 = r.y - py, rv2 = r.z - pz;
-                    double rr = cutoff_r2(r.x, r.y, r.z, px, py, pz);
+                    const float4 r = __ldg(env.rec + j);
+                    const float rv0 = r.x - px, rv1 = r.y - py, rv2 = r.z - pz;
+                    const double rr = cutoff_r2(r.x, r.y, r.z, px, py, pz);
                     if (rr < 64.0) {
-                        int tj = (int)r.w;
+                        const int tj = (int)r.w;
                         float rn = sqrtf((float)rr), fdr;
                         e_atom += eval_ef(rn - (r1 + vdw(tj)), ti, tj, fdr);
                         if (rn < EPS_F) rn = EPS_F;
@@ -404,22 +460,23 @@ __device__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* 
         F[3 * i] = fx; F[3 * i + 1] = fy; F[3 * i + 2] = fz;
     }
     __syncwarp();
-    // intra (bfgs.cuh:305-352)
+    // intra (bfgs.cuh:305-352): per-atom adjacency in both directions, per-pair curl;
+    // entries carry the pair flags, hydrogen pairs are marked and contribute nothing
     float e_intra = 0.f;
     for (int i = lane; i < T.natom; i += WARP) {
-        int ti = T.types[i];
-        float r1 = vdw(ti);
-        float xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
+        const float r1 = T.radius(i);
+        const float xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
         float fx = 0.f, fy = 0.f, fz = 0.f, ea = 0.f;
-        int k1 = T.pair_off[i + 1];
-        for (int k = T.pair_off[i]; k < k1; k++) {
-            int j = T.pairs[k];
-            float rv0 = X[3 * j] - xi, rv1 = X[3 * j + 1] - yi, rv2 = X[3 * j + 2] - zi;
-            float rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
+        const int k1 = T.pair_off(i + 1);
+        for (int k = T.pair_off(i); k < k1; k++) {
+            const int ent = T.pair(k);
+            if (ent & PAIR_ZERO) continue;
+            const int j = ent & 0xFFFF;
+            const float rv0 = X[3 * j] - xi, rv1 = X[3 * j + 1] - yi, rv2 = X[3 * j + 2] - zi;
+            const float rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
             if (rr < 64.f) {
-                int tj = T.types[j];
                 float rn = sqrtf(rr), fdr;
-                float ep = eval_ef(rn - (r1 + vdw(tj)), ti, tj, fdr);
+                float ep = vina_ef(rn - (r1 + T.radius(j)), ent & PAIR_HYD, ent & PAIR_HB, fdr);
                 if (rn < EPS_F) rn = EPS_F;
                 fdr /= rn;
                 float px = -fdr * rv0, py = -fdr * rv1, pz = -fdr * rv2;
@@ -441,31 +498,31 @@ __device__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* 
     if (env.bias_type != 0 && T.nbias > 0) {
         __syncwarp();
         for (int i = lane; i < T.natom; i += WARP) {
-            int b0 = T.bias_off[i], b1 = T.bias_off[i + 1];
+            const int b0 = T.bias_off(i), b1 = T.bias_off(i + 1);
             if (b0 < b1) {
-                float fb[3] = {0.f, 0.f, 0.f};
-                float px = X[3 * i], py = X[3 * i + 1], pz = X[3 * i + 2];
+                float fb0 = 0.f, fb1 = 0.f, fb2 = 0.f;
+                const float px = X[3 * i], py = X[3 * i + 1], pz = X[3 * i + 2];
                 for (int b = b0; b < b1; b++) {
-                    const float* bp = T.bias + 5 * b;
-                    float r[3] = {bp[0] - px, bp[1] - py, bp[2] - pz};
+                    const float* bp = T.bias() + 5 * b;
+                    const float r0 = bp[0] - px, r1 = bp[1] - py, r2 = bp[2] - pz;
                     if (env.bias_type == 1) {
-                        float rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                        float rr = r0 * r0 + r1 * r1 + r2 * r2;
                         float eb = bp[3] * env.bias_k * expf(-rr / bp[4]);
-                        fb[0] += eb * 2.f * r[0] / bp[4];
-                        fb[1] += eb * 2.f * r[1] / bp[4];
-                        fb[2] += eb * 2.f * r[2] / bp[4];
+                        fb0 += eb * 2.f * r0 / bp[4];
+                        fb1 += eb * 2.f * r1 / bp[4];
+                        fb2 += eb * 2.f * r2 / bp[4];
                         energy += eb;
                     } else {
-                        float ka = T.types[i] == VN_H ? 0.1f : 30.f;
-                        float rn = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+                        float ka = T.type(i) == VN_H ? 0.1f : 30.f;
+                        float rn = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
                         float ei = expf(3.f * (1.f - rn));
                         float eb = bp[3] * env.bias_k * ka / (1.f + ei);
                         float f = -eb * ei / (1.f + ei) * 3.f;
-                        fb[0] += f * r[0] / rn; fb[1] += f * r[1] / rn; fb[2] += f * r[2] / rn;
+                        fb0 += f * r0 / rn; fb1 += f * r1 / rn; fb2 += f * r2 / rn;
                         energy += eb;
                     }
                 }
-                F[3 * i] += fb[0]; F[3 * i + 1] += fb[1]; F[3 * i + 2] += fb[2];
+                F[3 * i] += fb0; F[3 * i + 1] += fb1; F[3 * i + 2] += fb2;
             }
         }
     }
@@ -474,24 +531,23 @@ __device__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* 
 }
 
 // Generalised gradient from per-atom dE/dx (bfgs.cuh:69-193).  G has 6+ntors entries.
-__device__ void grad_from_forces(const Topo& T, const Env& env, Slot P, const float* F, float* G) {
+__device__ __forceinline__ void grad_from_forces(const Topo& T, const Env& env, Slot P, const float* F, float* G) {
     const int lane = lane_id();
     const float* X = P.x;
     for (int k = lane; k < T.ntors; k += WARP) {
-        int from = T.axis[2 * k], to = T.axis[2 * k + 1];
-        float xt = X[3 * to], yt = X[3 * to + 1], zt = X[3 * to + 2];
+        const int from = T.axis(2 * k), to = T.axis(2 * k + 1);
+        const float xt = X[3 * to], yt = X[3 * to + 1], zt = X[3 * to + 2];
         float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-        int q1 = T.rot_off[k + 1];
-        for (int q = T.rot_off[k]; q < q1; q++) {
-            int a = T.rot[q];
-            if (T.types[a] == VN_H) continue;
-            float t0 = X[3 * a] - xt, t1 = X[3 * a + 1] - yt, t2 = X[3 * a + 2] - zt;
-            float f0 = F[3 * a], f1 = F[3 * a + 1], f2 = F[3 * a + 2];
+        const int q1 = T.rh_off(k + 1);
+        for (int q = T.rh_off(k); q < q1; q++) {       // heavy rotated atoms, in order
+            const int a = T.rheavy(q);
+            const float t0 = X[3 * a] - xt, t1 = X[3 * a + 1] - yt, t2 = X[3 * a + 2] - zt;
+            const float f0 = F[3 * a], f1 = F[3 * a + 1], f2 = F[3 * a + 2];
             s0 += t1 * f2 - t2 * f1;
             s1 += t2 * f0 - t0 * f2;
             s2 += t0 * f1 - t1 * f0;
         }
-        float a0 = xt - X[3 * from], a1 = yt - X[3 * from + 1], a2 = zt - X[3 * from + 2];
+        const float a0 = xt - X[3 * from], a1 = yt - X[3 * from + 1], a2 = zt - X[3 * from + 2];
         G[6 + k] = (s0 * a0 + s1 * a1 + s2 * a2) / sqrtf(a0 * a0 + a1 * a1 + a2 * a2);
     }
     if (env.constraint) {
@@ -499,29 +555,33 @@ __device__ void grad_from_forces(const Topo& T, const Env& env, Slot P, const fl
         __syncwarp();
         return;
     }
-    float q[4];
-    rotvec_to_quat(P.h[4], P.h[5], P.h[6], q);
-    q[1] = -q[1]; q[2] = -q[2]; q[3] = -q[3];
-    float cx = P.h[1], cy = P.h[2], cz = P.h[3];
-    float fs0 = 0.f, fs1 = 0.f, fs2 = 0.f;
-    float m[9];
+    float q0, q1, q2, q3;
+    rotvec_to_quat(P.h[4], P.h[5], P.h[6], q0, q1, q2, q3);
+    q1 = -q1; q2 = -q2; q3 = -q3;
+    const float cx = P.h[1], cy = P.h[2], cz = P.h[3];
+    float a[16];
 #pragma unroll
-    for (int j = 0; j < 9; j++) m[j] = 0.f;
+    for (int j = 0; j < 16; j++) a[j] = 0.f;
     for (int h = lane; h < T.nheavy; h += WARP) {
-        int i = T.heavy[h];
+        const int i = T.heavy(h);
         float t0 = X[3 * i] - cx, t1 = X[3 * i + 1] - cy, t2 = X[3 * i + 2] - cz;
-        quat_rotate(q, t0, t1, t2);
-        float f0 = F[3 * i], f1 = F[3 * i + 1], f2 = F[3 * i + 2];
-        fs0 += f0; fs1 += f1; fs2 += f2;
-        m[0] += f0 * t0; m[1] += f0 * t1; m[2] += f0 * t2;
-        m[3] += f1 * t0; m[4] += f1 * t1; m[5] += f1 * t2;
-        m[6] += f2 * t0; m[7] += f2 * t1; m[8] += f2 * t2;
+        quat_rotate(q0, q1, q2, q3, t0, t1, t2);
+        const float f0 = F[3 * i], f1 = F[3 * i + 1], f2 = F[3 * i + 2];
+        a[0] += f0; a[1] += f1; a[2] += f2;
+        a[3] += f0 * t0; a[4] += f0 * t1; a[5] += f0 * t2;
+        a[6] += f1 * t0; a[7] += f1 * t1; a[8] += f1 * t2;
+        a[9] += f2 * t0; a[10] += f2 * t1; a[11] += f2 * t2;
     }
-    fs0 = warp_sum(fs0); fs1 = warp_sum(fs1); fs2 = warp_sum(fs2);
+    reduce_scatter16(a);
+    // value v lives in lane rs16_lane(v): gather the 12 sums to every lane
+    float s[12];
 #pragma unroll
-    for (int j = 0; j < 9; j++) m[j] = warp_sum(m[j]);
-    if (lane == 0) { G[0] = fs0; G[1] = fs1; G[2] = fs2; }
-    if (lane < 3) G[3 + lane] = frob_drdv(m, P.h[4], P.h[5], P.h[6], lane);
+    for (int v = 0; v < 12; v++) s[v] = __shfl_sync(FULL, a[0], rs16_lane(v));
+    if (lane < 3) {
+        G[lane] = lane == 0 ? s[0] : (lane == 1 ? s[1] : s[2]);
+        RotGradBasis B = rot_grad_basis(P.h[4], P.h[5], P.h[6]);
+        G[3 + lane] = frob_drdv(B, lane, s[3], s[4], s[5], s[6], s[7], s[8], s[9], s[10], s[11]);
+    }
     __syncwarp();
 }
 
@@ -533,35 +593,47 @@ __device__ __forceinline__ float eval_e_grad(const Topo& T, const Env& env, Slot
 }
 
 // ---------------------------------------------------------------- kinematics
-// One torsion increment (bfgs.cuh:443-549); the centre is refreshed by the caller.
-__device__ void apply_dihe(const Topo& T, Slot P, int k, float incr_raw) {
+__device__ __forceinline__ void refresh_center(const Topo& T, Slot P) {
     const int lane = lane_id();
-    float incr = 0.f, ax = 0.f, ay = 0.f, az = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    for (int i = lane; i < T.natom; i += WARP) { s0 += P.x[3 * i]; s1 += P.x[3 * i + 1]; s2 += P.x[3 * i + 2]; }
+    s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2);
+    __syncwarp();
     if (lane == 0) {
-        float inc = normalize_angle(incr_raw);
-        int r0 = T.range_off[k], nr = T.range_off[k + 1] - r0;
-        float t = normalize_angle(P.d[k] + inc);
-        float dn = clamp_by_ranges(t, T.ranges + 2 * r0, nr);
-        incr = dn - P.d[k];
-        P.d[k] = dn;
-        int from = T.axis[2 * k], to = T.axis[2 * k + 1];
-        tx = P.x[3 * to]; ty = P.x[3 * to + 1]; tz = P.x[3 * to + 2];
-        ax = tx - P.x[3 * from]; ay = ty - P.x[3 * from + 1]; az = tz - P.x[3 * from + 2];
-        float l = sqrtf(ax * ax + ay * ay + az * az);
-        if (l <= EPS_F) { ax = 1.f; ay = 0.f; az = 0.f; }
-        else { ax /= l; ay /= l; az /= l; }
+        P.h[1] = s0 / T.natom; P.h[2] = s1 / T.natom; P.h[3] = s2 / T.natom;
     }
-    incr = __shfl_sync(FULL, incr, 0);
-    ax = __shfl_sync(FULL, ax, 0); ay = __shfl_sync(FULL, ay, 0); az = __shfl_sync(FULL, az, 0);
-    tx = __shfl_sync(FULL, tx, 0); ty = __shfl_sync(FULL, ty, 0); tz = __shfl_sync(FULL, tz, 0);
-    float s, c;
-    sincosf(incr, &s, &c);
-    int q1 = T.rot_off[k + 1];
-    for (int q = T.rot_off[k] + lane; q < q1; q += WARP) {
-        int a = T.rot[q];
-        float v0 = P.x[3 * a] - tx, v1 = P.x[3 * a + 1] - ty, v2 = P.x[3 * a + 2] - tz;
-        float m = (1.f - c) * (ax * v0 + ay * v1 + az * v2);
-        float c0 = ay * v2 - az * v1, c1 = az * v0 - ax * v2, c2 = ax * v1 - ay * v0;
+    __syncwarp();
+}
+
+// New value of dihedral k after an increment (bfgs.cuh:455-471): returns the applied
+// increment and stores the clamped dihedral.
+__device__ __forceinline__ float dihedral_step(const Topo& T, Slot P, int k, float incr_raw) {
+    const float inc = normalize_angle(incr_raw);
+    const int r0 = T.range_off(k), nr = T.range_off(k + 1) - r0;
+    const float t = normalize_angle(P.d[k] + inc);
+    const float dn = clamp_by_ranges(t, T.ranges() + 2 * r0, nr);
+    const float applied = dn - P.d[k];
+    P.d[k] = dn;
+    return applied;
+}
+
+// Rotate the atoms of torsion k by the angle with sine s and cosine c about the axis
+// from->to through `to` (bfgs.cuh:477-527); all lanes read the axis atoms directly.
+__device__ __forceinline__ void rotate_torsion(const Topo& T, Slot P, int k, float s, float c) {
+    const int lane = lane_id();
+    const int from = T.axis(2 * k), to = T.axis(2 * k + 1);
+    const float tx = P.x[3 * to], ty = P.x[3 * to + 1], tz = P.x[3 * to + 2];
+    float ax = tx - P.x[3 * from], ay = ty - P.x[3 * from + 1], az = tz - P.x[3 * from + 2];
+    const float l = sqrtf(ax * ax + ay * ay + az * az);
+    if (l <= EPS_F) { ax = 1.f; ay = 0.f; az = 0.f; }
+    else { ax /= l; ay /= l; az /= l; }
+    __syncwarp();
+    const int q1 = T.rot_off(k + 1);
+    for (int q = T.rot_off(k) + lane; q < q1; q += WARP) {
+        const int a = T.rot(q);
+        const float v0 = P.x[3 * a] - tx, v1 = P.x[3 * a + 1] - ty, v2 = P.x[3 * a + 2] - tz;
+        const float m = (1.f - c) * (ax * v0 + ay * v1 + az * v2);
+        const float c0 = ay * v2 - az * v1, c1 = az * v0 - ax * v2, c2 = ax * v1 - ay * v0;
         P.x[3 * a] = c * v0 + m * ax + s * c0 + tx;
         P.x[3 * a + 1] = c * v1 + m * ay + s * c1 + ty;
         P.x[3 * a + 2] = c * v2 + m * az + s * c2 + tz;
@@ -569,29 +641,41 @@ __device__ void apply_dihe(const Topo& T, Slot P, int k, float incr_raw) {
     __syncwarp();
 }
 
-__device__ void refresh_center(const Topo& T, Slot P) {
-    const int lane = lane_id();
-    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-    for (int i = lane; i < T.natom; i += WARP) { s0 += P.x[3 * i]; s1 += P.x[3 * i + 1]; s2 += P.x[3 * i + 2]; }
-    s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2);
-    if (lane == 0) {
-        P.h[1] = s0 / T.natom; P.h[2] = s1 / T.natom; P.h[3] = s2 / T.natom;
-    }
+// One torsion increment as the reference applies it (dihedral, rotation, centre).
+__device__ __forceinline__ void apply_dihe(const Topo& T, Slot P, int k, float incr_raw) {
+    float applied = 0.f;
+    if (lane_id() == 0) applied = dihedral_step(T, P, k, incr_raw);
+    applied = __shfl_sync(FULL, applied, 0);
     __syncwarp();
+    float s, c;
+    sincosf(applied, &s, &c);
+    rotate_torsion(T, P, k, s, c);
+    refresh_center(T, P);
 }
 
 // pose += alpha * g: torsions in index order, then rotation about the old centre and
-// translation (bfgs.cuh:560-618)
-__device__ void apply_update(const Topo& T, const Env& env, Slot P, const float* G, float alpha) {
-    for (int k = 0; k < T.ntors; k++) apply_dihe(T, P, k, G[6 + k] * alpha);
+// translation (bfgs.cuh:560-618).  SC holds 2 floats per torsion of scratch.  The
+// dihedral updates are independent of the coordinates, so they run lane-parallel first;
+// the rotations then follow sequentially in index order as in the reference.
+__device__ __forceinline__ void apply_update(const Topo& T, const Env& env, Slot P, const float* G, float alpha,
+                                             float* SC) {
+    const int lane = lane_id();
+    for (int k = lane; k < T.ntors; k += WARP) {
+        const float applied = dihedral_step(T, P, k, G[6 + k] * alpha);
+        float s, c;
+        sincosf(applied, &s, &c);
+        SC[2 * k] = s;
+        SC[2 * k + 1] = c;
+    }
+    __syncwarp();
+    for (int k = 0; k < T.ntors; k++) rotate_torsion(T, P, k, SC[2 * k], SC[2 * k + 1]);
     if (T.ntors > 0) refresh_center(T, P);
     if (env.constraint) return;
-    const int lane = lane_id();
-    float c0x = P.h[1], c0y = P.h[2], c0z = P.h[3];
-    float ncx = c0x + alpha * G[0], ncy = c0y + alpha * G[1], ncz = c0z + alpha * G[2];
-    float rx = G[3] * alpha, ry = G[4] * alpha, rz = G[5] * alpha;
-    float q[4];
-    rotvec_to_quat(rx, ry, rz, q);
+    const float c0x = P.h[1], c0y = P.h[2], c0z = P.h[3];
+    const float ncx = c0x + alpha * G[0], ncy = c0y + alpha * G[1], ncz = c0z + alpha * G[2];
+    const float rx = G[3] * alpha, ry = G[4] * alpha, rz = G[5] * alpha;
+    float q0, q1, q2, q3;
+    rotvec_to_quat(rx, ry, rz, q0, q1, q2, q3);
     __syncwarp();
     if (lane == 0) {
         P.h[1] = ncx; P.h[2] = ncy; P.h[3] = ncz;
@@ -599,7 +683,7 @@ __device__ void apply_update(const Topo& T, const Env& env, Slot P, const float*
     }
     for (int i = lane; i < T.natom; i += WARP) {
         float v0 = P.x[3 * i] - c0x, v1 = P.x[3 * i + 1] - c0y, v2 = P.x[3 * i + 2] - c0z;
-        quat_rotate(q, v0, v1, v2);
+        quat_rotate(q0, q1, q2, q3, v0, v1, v2);
         P.x[3 * i] = v0 + ncx; P.x[3 * i + 1] = v1 + ncy; P.x[3 * i + 2] = v2 + ncz;
     }
     __syncwarp();
@@ -613,7 +697,8 @@ struct Work {        // per-warp scratch in shared memory
     float* p;        // D
     float* y;        // D
     float* mhy;      // D
-    double* H;       // D(D+1)/2
+    float* sc;       // 2T torsion sine/cosine scratch
+    double* H;       // D(D+1)/2, packed upper triangle: H[i + j(j+1)/2], i <= j
 };
 
 __device__ __forceinline__ float gdot(const float* a, const float* b, int n) {
@@ -622,16 +707,27 @@ __device__ __forceinline__ float gdot(const float* a, const float* b, int n) {
     return warp_sum(s);
 }
 
-__device__ __forceinline__ int tri(int i, int j) { return i <= j ? i + j * (j + 1) / 2 : j + i * (i + 1) / 2; }
+// out = -H v for the packed symmetric H (bfgs.cuh:413-428), lane per row
+__device__ __forceinline__ void minus_hv(const double* H, const float* v, float* out, int dim) {
+    for (int i = lane_id(); i < dim; i += WARP) {
+        double s = 0.0;
+        const int ri = i * (i + 1) / 2;
+        for (int j = 0; j < i; j++) s += H[ri + j] * (double)v[j];              // H[j,i], j < i
+        for (int j = i, cj = ri; j < dim; cj += j + 1, j++) s += H[cj + i] * (double)v[j];  // H[i,j], j >= i
+        out[i] = (float)(-s);
+    }
+    __syncwarp();
+}
 
 // Backtracking Armijo line search (bfgs.cuh:623-670).  Trial poses go to Pn.
-__device__ float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, const Work& W, int dim,
-                             float e0, float vcap, float slope, float& alpha_out, int& n_eval) {
+__device__ __forceinline__ float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, const Work& W,
+                                             int dim, float e0, float vcap, float slope, float& alpha_out,
+                                             int& n_eval) {
     float alpha = 1.f, e_new = 0.f;
-    float pg = gdot(W.p, W.g, dim);
+    const float pg = gdot(W.p, W.g, dim);
     for (int trial = 0; trial < LS_STEPS; trial++) {
         slot_copy(Pn, Px, T.natom, T.ntors);
-        apply_update(T, env, Pn, W.p, alpha);
+        apply_update(T, env, Pn, W.p, alpha, W.sc);
         e_new = eval_e_grad(T, env, Pn, W.F, W.gn, vcap, slope);
         n_eval++;
         if (e_new - e0 < 1e-4f * alpha * pg) break;
@@ -641,14 +737,14 @@ __device__ float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, co
     return e_new;
 }
 
-// BFGS on the pose in slot ix (bfgs.cuh:729-829).  Uses slots in / alt / ori; returns
+// BFGS on the pose in slot ix (bfgs.cuh:729-829).  Uses slots ix / ialt / iori; returns
 // the slot index holding the result, whose header[0] is the final energy.
-__device__ int bfgs(const Topo& T, const Env& env, float* slots, int stride, int ix, int ialt, int iori,
-                    const Work& W, int max_steps, float vcap, float slope, int& n_eval) {
+__device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots, int stride, int ix, int ialt,
+                                    int iori, const Work& W, int max_steps, float vcap, float slope, int& n_eval) {
     const int lane = lane_id();
     const int dim = 6 + T.ntors;
-    Slot X = slot_at(slots, stride, ix, T.natom);
-    float E_ori = eval_e_grad(T, env, X, W.F, W.g, vcap, slope);
+    const Slot X = slot_at(slots, stride, ix, T.natom);
+    const float E_ori = eval_e_grad(T, env, X, W.F, W.g, vcap, slope);
     n_eval++;
     float E = E_ori;
     const int ntri = dim * (dim + 1) / 2;
@@ -658,57 +754,45 @@ __device__ int bfgs(const Topo& T, const Env& env, float* slots, int stride, int
     slot_copy(slot_at(slots, stride, iori, T.natom), X, T.natom, T.ntors);
     int cur = ix, alt = ialt;
     for (int step = 0; step < max_steps; step++) {
-        // p = -H g
-        for (int i = lane; i < dim; i += WARP) {
-            double s = 0.0;
-            for (int j = 0; j < dim; j++) s += W.H[tri(i, j)] * (double)W.g[j];
-            W.p[i] = (float)(-s);
-        }
-        __syncwarp();
+        minus_hv(W.H, W.g, W.p, dim);                         // p = -H g
         float alpha;
-        Slot Pc = slot_at(slots, stride, cur, T.natom);
-        Slot Pa = slot_at(slots, stride, alt, T.natom);
-        float E1 = line_search(T, env, Pc, Pa, W, dim, E, vcap, slope, alpha, n_eval);
+        const float E1 = line_search(T, env, slot_at(slots, stride, cur, T.natom),
+                                     slot_at(slots, stride, alt, T.natom), W, dim, E, vcap, slope, alpha, n_eval);
         for (int i = lane; i < dim; i += WARP) W.y[i] = W.gn[i] - W.g[i];
         __syncwarp();
         E = E1;
-        int t = cur; cur = alt; alt = t;       // x := x_new
-        float gg = gdot(W.g, W.g, dim);
+        const int t = cur; cur = alt; alt = t;                // x := x_new
+        const float gg = gdot(W.g, W.g, dim);                 // the reference tests the old gradient
         if (sqrtf(gg) < 1e-5f) break;
         for (int i = lane; i < dim; i += WARP) W.g[i] = W.gn[i];
         __syncwarp();
         if (step == 0) {
-            float yy = gdot(W.y, W.y, dim);
+            const float yy = gdot(W.y, W.y, dim);
             if (fabsf(yy) > EPS_F) {
-                float yp0 = gdot(W.y, W.p, dim);
+                const float yp0 = gdot(W.y, W.p, dim);
                 for (int i = lane; i < dim; i += WARP) W.H[i + i * (i + 1) / 2] = (double)(alpha * yp0 / yy);
                 __syncwarp();
             }
         }
-        float yp = gdot(W.y, W.p, dim);
+        const float yp = gdot(W.y, W.p, dim);
         if (alpha * yp < EPS_F) continue;
-        for (int i = lane; i < dim; i += WARP) {
-            double s = 0.0;
-            for (int j = 0; j < dim; j++) s += W.H[tri(i, j)] * (double)W.y[j];
-            W.mhy[i] = (float)(-s);
-        }
-        __syncwarp();
-        double yhy = -(double)gdot(W.y, W.mhy, dim);
-        double r = 1.0 / ((double)alpha * (double)yp);
-        double a = alpha;
-        double c2 = a * a * (r * r * yhy + r);
+        minus_hv(W.H, W.y, W.mhy, dim);
+        const double yhy = -(double)gdot(W.y, W.mhy, dim);
+        const double r = 1.0 / ((double)alpha * (double)yp);
+        const double a = alpha;
+        const double c1 = a * r, c2 = a * a * (r * r * yhy + r);
         for (int idx = lane; idx < ntri; idx += WARP) {
-            // packed upper triangle: idx = i + j(j+1)/2 with i <= j
-            int j = (int)((sqrtf(8.f * idx + 1.f) - 1.f) * 0.5f);
-            while (j * (j + 1) / 2 > idx) j--;
-            while ((j + 1) * (j + 2) / 2 <= idx) j++;
-            int i = idx - j * (j + 1) / 2;
-            double pi = W.p[i], pj = W.p[j];
-            W.H[idx] += a * r * ((double)W.mhy[i] * pj + (double)W.mhy[j] * pi) + c2 * pi * pj;
+            // idx = i + j(j+1)/2, i <= j
+            int j = (int)((sqrtf(8.f * (float)idx + 1.f) - 1.f) * 0.5f);
+            j -= (j * (j + 1) / 2 > idx);
+            j += ((j + 1) * (j + 2) / 2 <= idx);
+            const int i = idx - j * (j + 1) / 2;
+            const double pi = W.p[i], pj = W.p[j];
+            W.H[idx] += c1 * ((double)W.mhy[i] * pj + (double)W.mhy[j] * pi) + c2 * pi * pj;
         }
         __syncwarp();
     }
-    Slot R = slot_at(slots, stride, cur, T.natom);
+    const Slot R = slot_at(slots, stride, cur, T.natom);
     if (E > E_ori) {
         E = E_ori;
         slot_copy(R, slot_at(slots, stride, iori, T.natom), T.natom, T.ntors);
@@ -719,99 +803,94 @@ __device__ int bfgs(const Topo& T, const Env& env, float* slots, int stride, int
 }
 
 // ---------------------------------------------------------------- MC moves
-__device__ float gyration_radius(const Topo& T, Slot P) {
+__device__ __forceinline__ float gyration_radius(const Topo& T, Slot P) {
     const int lane = lane_id();
     float s = 0.f;
     for (int h = lane; h < T.nheavy; h += WARP) {
-        int i = T.heavy[h];
-        float d0 = P.x[3 * i] - P.h[1], d1 = P.x[3 * i + 1] - P.h[2], d2 = P.x[3 * i + 2] - P.h[3];
+        const int i = T.heavy(h);
+        const float d0 = P.x[3 * i] - P.h[1], d1 = P.x[3 * i + 1] - P.h[2], d2 = P.x[3 * i + 2] - P.h[3];
         s += d0 * d0 + d1 * d1 + d2 * d2;
     }
     s = warp_sum(s);
-    float r = T.nheavy > 0 ? sqrtf(s / T.nheavy) : 0.f;
+    const float r = T.nheavy > 0 ? sqrtf(s / T.nheavy) : 0.f;
     return r > 0.f ? r : 1.f;
 }
 
-__device__ __forceinline__ void rand_in_sphere(const Rng& rng, uint32_t step, float* v) {
+__device__ __forceinline__ void rand_in_sphere(const Rng& rng, uint32_t step, float& v0, float& v1, float& v2) {
     for (int a = 0; a < 64; a++) {
-        U4 u = rng.draw(step, P_SPHERE + a);
-        v[0] = (u01(u.x) - 0.5f) * 2.f;
-        v[1] = (u01(u.y) - 0.5f) * 2.f;
-        v[2] = (u01(u.z) - 0.5f) * 2.f;
-        if (sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) < 1.f) return;
+        const U4 u = rng.draw(step, P_SPHERE + a);
+        v0 = (u01(u.x) - 0.5f) * 2.f;
+        v1 = (u01(u.y) - 0.5f) * 2.f;
+        v2 = (u01(u.z) - 0.5f) * 2.f;
+        if (sqrtf(v0 * v0 + v1 * v1 + v2 * v2) < 1.f) return;
     }
-    v[0] = v[1] = v[2] = 0.f;
+    v0 = v1 = v2 = 0.f;
 }
 
 // mc.cu:146-256 with the counter-based generator
-__device__ void mutate(const Topo& T, const Env& env, const Rng& rng, uint32_t step, Slot P) {
+__device__ __forceinline__ void mutate(const Topo& T, const Env& env, const Rng& rng, uint32_t step, Slot P) {
     const int lane = lane_id();
     const float amp = 2.f;
-    int nmut = 2 + T.ntors;
-    U4 u = rng.draw(step, P_WHICH);
+    const int nmut = 2 + T.ntors;
+    const U4 u = rng.draw(step, P_WHICH);
     int which;
     if (env.constraint) which = nmut < 3 ? 3 : 2 + (int)(u.x % (uint32_t)(nmut - 2));
     else which = (int)(u.x % (uint32_t)nmut);
     if (which == 0) {
-        float v[3];
-        rand_in_sphere(rng, step, v);
-        float d[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            float c = P.h[1 + a];
-            float t = amp * v[a] + c;
-            if (t > env.box_hi[a]) t = env.box_hi[a];
-            if (t < env.box_lo[a]) t = env.box_lo[a];
-            d[a] = t - c;
-        }
+        float v0, v1, v2;
+        rand_in_sphere(rng, step, v0, v1, v2);
+        const float c0 = P.h[1], c1 = P.h[2], c2 = P.h[3];
+        const float t0 = fminf(fmaxf(amp * v0 + c0, env.box_lo[0]), env.box_hi[0]);
+        const float t1 = fminf(fmaxf(amp * v1 + c1, env.box_lo[1]), env.box_hi[1]);
+        const float t2 = fminf(fmaxf(amp * v2 + c2, env.box_lo[2]), env.box_hi[2]);
+        const float d0 = t0 - c0, d1 = t1 - c1, d2 = t2 - c2;
         __syncwarp();
-        if (lane == 0) { P.h[1] += d[0]; P.h[2] += d[1]; P.h[3] += d[2]; }
+        if (lane == 0) { P.h[1] = c0 + d0; P.h[2] = c1 + d1; P.h[3] = c2 + d2; }
         for (int i = lane; i < T.natom; i += WARP) {
-            P.x[3 * i] += d[0]; P.x[3 * i + 1] += d[1]; P.x[3 * i + 2] += d[2];
+            P.x[3 * i] += d0; P.x[3 * i + 1] += d1; P.x[3 * i + 2] += d2;
         }
         __syncwarp();
     } else if (which == 1) {
-        float v[3];
-        rand_in_sphere(rng, step, v);
-        float a = gyration_radius(T, P);
-        float rv[3] = {amp / a * v[0], amp / a * v[1], amp / a * v[2]};
-        float q[4];
-        rotvec_to_quat(rv[0], rv[1], rv[2], q);
-        float cx = P.h[1], cy = P.h[2], cz = P.h[3];
+        float v0, v1, v2;
+        rand_in_sphere(rng, step, v0, v1, v2);
+        const float a = gyration_radius(T, P);
+        const float rv0 = amp / a * v0, rv1 = amp / a * v1, rv2 = amp / a * v2;
+        float q0, q1, q2, q3;
+        rotvec_to_quat(rv0, rv1, rv2, q0, q1, q2, q3);
+        const float cx = P.h[1], cy = P.h[2], cz = P.h[3];
         __syncwarp();
-        if (lane == 0) { P.h[4] = rv[0]; P.h[5] = rv[1]; P.h[6] = rv[2]; }
+        if (lane == 0) { P.h[4] = rv0; P.h[5] = rv1; P.h[6] = rv2; }
         for (int i = lane; i < T.natom; i += WARP) {
             float t0 = P.x[3 * i] - cx, t1 = P.x[3 * i + 1] - cy, t2 = P.x[3 * i + 2] - cz;
-            quat_rotate(q, t0, t1, t2);
+            quat_rotate(q0, q1, q2, q3, t0, t1, t2);
             P.x[3 * i] = t0 + cx; P.x[3 * i + 1] = t1 + cy; P.x[3 * i + 2] = t2 + cz;
         }
         __syncwarp();
     } else if (which - 2 < T.ntors) {
-        int k = which - 2;
-        U4 w = rng.draw(step, P_TORS);
-        float r0 = u01(w.x), r1 = u01(w.y);
-        int b = T.range_off[k], nr = T.range_off[k + 1] - b;
+        const int k = which - 2;
+        const U4 w = rng.draw(step, P_TORS);
+        const float r0 = u01(w.x), r1 = u01(w.y);
+        const int b = T.range_off(k), nr = T.range_off(k + 1) - b;
         int ir = (int)ceilf(r0 * nr - 1.f);
         ir = ir < 0 ? 0 : (ir > nr - 1 ? nr - 1 : ir);
-        float lo = T.ranges[2 * (b + ir)], hi = T.ranges[2 * (b + ir) + 1];
-        float a = lo + (hi - lo) * r1 - P.d[k];
+        const float lo = T.ranges()[2 * (b + ir)], hi = T.ranges()[2 * (b + ir) + 1];
+        const float a = lo + (hi - lo) * r1 - P.d[k];
         apply_dihe(T, P, k, a);
-        refresh_center(T, P);
     }
 }
 
-// initial randomisation (mc.cu:18-104); G is D floats of scratch
-__device__ void randomize(const Topo& T, const Env& env, const Rng& rng, int chain, int nchain, Slot P, float* G) {
+// initial randomisation (mc.cu:18-104); G is D floats of scratch, SC 2T floats
+__device__ __forceinline__ void randomize(const Topo& T, const Env& env, const Rng& rng, int chain, int nchain,
+                                          Slot P, float* G, float* SC) {
     const int lane = lane_id();
     if (lane == 0) {
-        U4 u = rng.draw(0, P_INIT);
+        const U4 u = rng.draw(0, P_INIT);
         if (env.constraint) {
             G[0] = G[1] = G[2] = G[3] = G[4] = G[5] = 0.f;
         } else {
-            float s = chain + 0.5f, n = (float)nchain;
-            float r = sqrtf(s / n), R = sqrtf(1.f - s / n);
-            float al = 2.f * PI_F * s / 1.4142136f, be = 2.f * PI_F * s / 1.5337512f;
-            float q[4] = {r * sinf(al), r * cosf(al), R * sinf(be), R * cosf(be)};
+            const float s = chain + 0.5f, n = (float)nchain;
+            const float r = sqrtf(s / n), R = sqrtf(1.f - s / n);
+            const float al = 2.f * PI_F * s / 1.4142136f, be = 2.f * PI_F * s / 1.5337512f;
             if (env.bias_type == 2) {
                 G[0] = G[1] = G[2] = 0.f;
             } else {
@@ -819,19 +898,19 @@ __device__ void randomize(const Topo& T, const Env& env, const Rng& rng, int cha
                 G[1] = (env.box_lo[1] + (env.box_hi[1] - env.box_lo[1]) * u01(u.y)) - P.h[2];
                 G[2] = (env.box_lo[2] + (env.box_hi[2] - env.box_lo[2]) * u01(u.z)) - P.h[3];
             }
-            quat_to_rotvec(q, G + 3);
+            quat_to_rotvec(r * sinf(al), r * cosf(al), R * sinf(be), R * cosf(be), G + 3);
         }
     }
     for (int k = lane; k < T.ntors; k += WARP) {
-        U4 u = rng.draw(0, P_INIT + 1 + k);
-        int b = T.range_off[k], nr = T.range_off[k + 1] - b;
+        const U4 u = rng.draw(0, P_INIT + 1 + k);
+        const int b = T.range_off(k), nr = T.range_off(k + 1) - b;
         int j = (int)(u01(u.x) * nr);
         if (j > nr - 1) j = nr - 1;
-        float lo = T.ranges[2 * (b + j)], hi = T.ranges[2 * (b + j) + 1];
+        const float lo = T.ranges()[2 * (b + j)], hi = T.ranges()[2 * (b + j) + 1];
         G[6 + k] = lo + (hi - lo) * u01(u.y) - P.d[k];
     }
     __syncwarp();
-    apply_update(T, env, P, G, 1.f);
+    apply_update(T, env, P, G, 1.f, SC);
 }
 
 }  // namespace ud

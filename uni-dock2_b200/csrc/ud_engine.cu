@@ -24,12 +24,16 @@
 
 using namespace ud;
 
+// XS-type vdW radii on the host (src/constants/constants.h:21-43)
+static const float kVdwHost[NT] = {1.1f, 1.92f, 1.9f, 1.9f, 1.8f, 1.8f, 1.8f, 1.8f, 1.7f, 1.7f, 1.7f,
+                                   1.7f, 1.5f, 2.2f, 2.1f, 2.0f, 1.8f, 2.0f, 2.2f, 2.3f, 1.2f};
+
 // ====================================================================== layout helpers
 __host__ __device__ inline int r4(int x) { return (x + 3) & ~3; }
 __host__ __device__ inline int rec_floats(int n, int t) { return r4(8 + 3 * n + t); }
 __host__ __device__ inline int ws_floats(int n, int t) {
     int d = 6 + t;
-    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(d * (d + 1));
+    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(2 * t) + r4(d * (d + 1));
 }
 
 struct LigDev {
@@ -52,7 +56,8 @@ __device__ __forceinline__ Work work_at(float* ws, int natom, int ntors) {
     W.p = W.gn + r4(d);
     W.y = W.p + r4(d);
     W.mhy = W.y + r4(d);
-    W.H = reinterpret_cast<double*>(W.mhy + r4(d));
+    W.sc = W.mhy + r4(d);
+    W.H = reinterpret_cast<double*>(W.sc + r4(2 * ntors));
     return W;
 }
 
@@ -178,19 +183,19 @@ __global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict_
     const float* X = xyz + xoff[pose];
     float e_intra = 0.f, e_inter = 0.f, e_pen = 0.f, e_bias = 0.f;
     for (int i = lane; i < T.natom; i += WARP) {
-        int ti = T.types[i];
+        int ti = T.type(i);
         float xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
-        for (int k = T.pair_off[i]; k < T.pair_off[i + 1]; k++) {
-            int j = T.pairs[k];
+        for (int k = T.pair_off(i); k < T.pair_off(i + 1); k++) {
+            int j = T.pair(k) & 0xFFFF;
             if (j <= i) continue;
             float d0 = X[3 * j] - xi, d1 = X[3 * j + 1] - yi, d2 = X[3 * j + 2] - zi;
             float rr = d0 * d0 + d1 * d1 + d2 * d2;
-            if (rr < 64.f) e_intra += eval_e(sqrtf(rr) - (vdw(ti) + vdw(T.types[j])), ti, T.types[j]);
+            if (rr < 64.f) e_intra += eval_e(sqrtf(rr) - (vdw(ti) + vdw(T.type(j))), ti, T.type(j));
         }
         if (ti == VN_H) continue;
         float dec[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
         if (env.mode == 1) {
-            int m = env.map_of_type[ti];
+            int m = T.map_index(i);
             float gx, gy, gz;
             if (m >= 0) e_inter += grid_sample(env.grid, m, xi, yi, zi, gx, gy, gz);
         } else {
@@ -230,19 +235,19 @@ __global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict_
     }
     if (decomp) {  // hydrogens get zero rows
         for (int i = lane; i < T.natom; i += WARP)
-            if (T.types[i] == VN_H)
+            if (T.type(i) == VN_H)
                 for (int q = 0; q < 5; q++) decomp[doff[pose] + 5 * i + q] = 0.f;
     }
     if (env.bias_type != 0) {
         for (int i = lane; i < T.natom; i += WARP) {
-            for (int b = T.bias_off[i]; b < T.bias_off[i + 1]; b++) {
-                const float* bp = T.bias + 5 * b;
+            for (int b = T.bias_off(i); b < T.bias_off(i + 1); b++) {
+                const float* bp = T.bias() + 5 * b;
                 float r[3] = {bp[0] - X[3 * i], bp[1] - X[3 * i + 1], bp[2] - X[3 * i + 2]};
                 if (env.bias_type == 1) {
                     float rr = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
                     e_bias += bp[3] * env.bias_k * expf(-rr / bp[4]);
                 } else {
-                    float ka = T.types[i] == VN_H ? 0.1f : 30.f;
+                    float ka = T.type(i) == VN_H ? 0.1f : 30.f;
                     float rn = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
                     float ei = expf(3.f * (1.f - rn));
                     e_bias += bp[3] * env.bias_k * ka / (1.f + ei);
@@ -302,7 +307,7 @@ __device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp,
 
 __device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
 
-__global__ void __launch_bounds__(256) k_search(const int* __restrict__ blobs, const LigDev* __restrict__ ligs,
+__global__ void __launch_bounds__(256, 3) k_search(const int* __restrict__ blobs, const LigDev* __restrict__ ligs,
                                                 const int* __restrict__ order, int nlig, Env env, SearchP sp,
                                                 float* best, int* work_counter, unsigned long long* nevals) {
     extern __shared__ __align__(16) float smem[];
@@ -333,7 +338,7 @@ __global__ void __launch_bounds__(256) k_search(const int* __restrict__ blobs, c
             int A = 0;
             Slot SA = slot_at(ws, L.stride, A, T.natom);
             load_initial(sblob, SA, T.natom, T.ntors);
-            if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g);
+            if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
             int ne = 0;
             float best_e = 1e9f;
             if (sp.mc_steps == 0) {
@@ -343,38 +348,43 @@ __global__ void __launch_bounds__(256) k_search(const int* __restrict__ blobs, c
                 __syncwarp();
                 store_record(out, SA, nrec);
             } else {
+                // slots: A holds the accepted pose; the other three serve the candidate and
+                // the optimiser.  Both BFGS runs of a step (candidate with curl 10, accepted
+                // new best with curl 1000) go through one call site (phase 0 / 1).
                 for (int step = 0; step < sp.mc_steps; step++) {
-                    int fr[3], k = 0;
-                    for (int s = 0; s < 4; s++) if (s != A) fr[k++] = s;
-                    Slot SC = slot_at(ws, L.stride, fr[0], T.natom);
+                    const int C = (A + 1) & 3;
+                    Slot SC = slot_at(ws, L.stride, C, T.natom);
                     slot_copy(SC, slot_at(ws, L.stride, A, T.natom), T.natom, T.ntors);
                     mutate(T, env, rng, (uint32_t)step, SC);
-                    int R = fr[0];
+                    const float e_acc = ws[A * L.stride];
+                    const float rx = u01(rng.draw((uint32_t)step, P_METRO).x);
                     if (sp.opt_steps == 0) {
                         float e = eval_e_grad(T, env, SC, W.F, W.g, VCAP_SEARCH, PENALTY_SLOPE);
                         ne++;
                         if (lane == 0) SC.h[0] = e;
                         __syncwarp();
-                    } else {
-                        R = bfgs(T, env, ws, L.stride, fr[0], fr[1], fr[2], W, sp.opt_steps, VCAP_SEARCH,
-                                 PENALTY_SLOPE, ne);
-                    }
-                    float e_acc = ws[(size_t)A * L.stride];
-                    float e_new = ws[(size_t)R * L.stride];
-                    U4 u = rng.draw((uint32_t)step, P_METRO);
-                    bool acc = metropolis(e_acc, e_new, 1.2f, u01(u.x));
-                    if (step == 0 || acc) {
-                        A = R;
-                        if (e_new < best_e) {
-                            if (sp.opt_steps > 0) {
-                                int g3[3], q = 0;
-                                for (int s = 0; s < 4; s++) if (s != A) g3[q++] = s;
-                                A = bfgs(T, env, ws, L.stride, A, g3[0], g3[1], W, sp.opt_steps, VCAP_AUTH,
-                                         PENALTY_SLOPE, ne);
+                        if (step == 0 || metropolis(e_acc, e, 1.2f, rx)) {
+                            A = C;
+                            if (e < best_e) {
+                                best_e = e;
+                                store_record(out, SC, nrec);
                             }
-                            float ea = ws[(size_t)A * L.stride];
-                            if (ea < best_e) {
-                                best_e = ea;
+                        }
+                        continue;
+                    }
+                    for (int phase = 0; phase < 2; phase++) {
+                        const int X = (A + 1 - phase) & 3;
+                        const int R = bfgs(T, env, ws, L.stride, X, (X + 1) & 3, (X + 2) & 3, W, sp.opt_steps,
+                                           phase ? VCAP_AUTH : VCAP_SEARCH, PENALTY_SLOPE, ne);
+                        const float e_new = ws[R * L.stride];
+                        if (phase == 0) {
+                            if (!(step == 0 || metropolis(e_acc, e_new, 1.2f, rx))) break;
+                            A = R;
+                            if (!(e_new < best_e)) break;
+                        } else {
+                            A = R;
+                            if (e_new < best_e) {
+                                best_e = e_new;
                                 store_record(out, slot_at(ws, L.stride, A, T.natom), nrec);
                             }
                         }
@@ -433,7 +443,7 @@ __global__ void k_cluster(const int* __restrict__ blobs, const LigDev* __restric
             const float* xl = base + (long long)lead[t] * L.stride + 8;
             float acc = 0.f;
             for (int h = 0; h < T.nheavy; h++) {
-                int a = T.heavy[h];
+                int a = T.heavy(h);
                 float dx = __fsub_rn(xc[3 * a], xl[3 * a]);
                 float dy = __fsub_rn(xc[3 * a + 1], xl[3 * a + 1]);
                 float dz = __fsub_rn(xc[3 * a + 2], xl[3 * a + 2]);
@@ -623,13 +633,16 @@ Env make_env(ud_ctx* c, int mode) {
     e.grid.ox = c->origin[0]; e.grid.oy = c->origin[1]; e.grid.oz = c->origin[2];
     e.grid.inv_s = c->spacing > 0 ? 1.f / c->spacing : 0.f;
     e.grid.gx = c->gdim[0]; e.grid.gy = c->gdim[1]; e.grid.gz = c->gdim[2];
-    memcpy(e.map_of_type, c->map_of_type, sizeof(e.map_of_type));
     if (mode == UD_MODE_GRID && c->nmaps == 0) throw Fail(UD_ESTATE, "grid mode requested but no grid was built");
     return e;
 }
 
 void sync_ligs(ud_ctx* c) {
     if (!c->ligs_dirty) return;
+    for (const LigHost& h : c->h_ligs) {       // per-atom grid map slot for the current maps
+        int* b = c->h_blobs.data() + h.blob_off;
+        for (int i = 0; i < h.natom; i++) b[b[H_MAPIDX] + i] = c->map_of_type[b[b[H_TYPES] + i]];
+    }
     c->d_blobs.upload(c->h_blobs.data(), c->h_blobs.size(), c->stream);
     c->h_ligdev.resize(c->h_ligs.size());
     for (size_t i = 0; i < c->h_ligs.size(); i++) {
@@ -775,6 +788,7 @@ int ud_build_grid(ud_ctx* c, float spacing, int nmaps, const int* map_types, int
         }
         c->spacing = spacing;
         c->nmaps = nmaps;
+        c->ligs_dirty = true;          // map slots of loaded ligands change
         long long npt = (long long)c->gdim[0] * c->gdim[1] * c->gdim[2];
         c->d_maps32.ensure((size_t)npt * nmaps);
         c->d_maps16.ensure((size_t)npt * nmaps);
@@ -870,10 +884,19 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
             o = put(H_PAIR_OFF, n + 1);
             for (int i = 0; i <= n; i++) blob[o + i] = pair_off[a0 + i] - p0;
             o = put(H_PAIRS, np);
-            for (int k = 0; k < np; k++) {
-                int v = pairs[p0 + k];
-                if (v < 0 || v >= n) throw Fail(UD_EINVAL, "intra pair atom out of range");
-                blob[o + k] = v;
+            for (int i = 0; i < n; i++) {
+                const int ti = types[a0 + i];
+                for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++) {
+                    int v = pairs[p0 + k];
+                    if (v < 0 || v >= n) throw Fail(UD_EINVAL, "intra pair atom out of range");
+                    const int tj = types[a0 + v];
+                    const unsigned b1 = 1u << ti, b2 = 1u << tj;
+                    int ent = v;
+                    if (ti == VN_H || tj == VN_H) ent |= PAIR_ZERO;
+                    if ((b1 & HYD_MASK) && (b2 & HYD_MASK)) ent |= PAIR_HYD;
+                    if (((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK))) ent |= PAIR_HB;
+                    blob[o + k] = ent;
+                }
             }
             o = put(H_BIAS_OFF, n + 1);
             for (int i = 0; i <= n; i++) blob[o + i] = bias_off ? bias_off[a0 + i] - b0 : 0;
@@ -893,6 +916,27 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 float cc[3] = {s[0] / n, s[1] / n, s[2] / n};
                 memcpy(&blob[o], cc, sizeof(cc));
             }
+            o = put(H_RADII, n);
+            for (int i = 0; i < n; i++) {
+                const float r = kVdwHost[types[a0 + i]];
+                memcpy(&blob[o + i], &r, sizeof(float));
+            }
+            {   // heavy rotated atoms per torsion, in the reference's loop order
+                std::vector<int> rh_off(T + 1, 0), rh;
+                for (int k = 0; k < T; k++) {
+                    for (int q = rot_off[t0 + k]; q < rot_off[t0 + k + 1]; q++) {
+                        const int a = rot_atoms[q];
+                        if (types[a0 + a] != VN_H) rh.push_back(a);
+                    }
+                    rh_off[k + 1] = (int)rh.size();
+                }
+                o = put(H_RHOFF, T + 1);
+                for (int k = 0; k <= T; k++) blob[o + k] = rh_off[k];
+                o = put(H_RHEAVY, (int)rh.size());
+                for (size_t q = 0; q < rh.size(); q++) blob[o + q] = rh[q];
+            }
+            o = put(H_MAPIDX, n);      // filled from the current grid at upload (sync_ligs)
+            for (int i = 0; i < n; i++) blob[o + i] = -1;
             blob[H_TOTAL] = (int)blob.size();
             LigHost h;
             h.natom = n; h.ntors = T; h.nheavy = nheavy;

@@ -188,15 +188,22 @@ def make_ligand(natom: int, ntors: int, seed: int, center: Sequence[float],
     the ligand then grows from that fixed rigid core, keeps the core's absolute
     placement, takes the core as its root, and its torsions are all outside the core.
     """
-    rng = np.random.default_rng(np.random.SeedSequence([seed, 0x11C]))
-    if core is not None:
-        k = len(core["xyz"])
-        xyz, bonds = _grow_tree(natom, rng, core=(np.asarray(core["xyz"], float), list(core["bonds"])))
-        elem = list(core["elements"]) + [None] * (natom - k)
+    for attempt in range(64):       # a random walk can box itself in: restart it
+        rng = np.random.default_rng(np.random.SeedSequence([seed, 0x11C, attempt]))
+        try:
+            if core is not None:
+                k = len(core["xyz"])
+                xyz, bonds = _grow_tree(natom, rng, core=(np.asarray(core["xyz"], float), list(core["bonds"])))
+                elem = list(core["elements"]) + [None] * (natom - k)
+            else:
+                k = 0
+                xyz, bonds = _grow_tree(natom, rng)
+                elem = [None] * natom
+            break
+        except RuntimeError:
+            continue
     else:
-        k = 0
-        xyz, bonds = _grow_tree(natom, rng)
-        elem = [None] * natom
+        raise RuntimeError("ligand growth failed")
     for i in range(natom):
         if elem[i] is None:
             r = rng.random()
