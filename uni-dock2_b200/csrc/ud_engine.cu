@@ -293,6 +293,10 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
 }
 
 // ====================================================================== MC search
+#ifndef SEARCH_MIN_BLOCKS
+#define SEARCH_MIN_BLOCKS 4          // 256-thread CTAs per SM the register budget is sized for
+#endif
+constexpr int SEARCH_ITEM_CHAINS = 16;
 struct SearchP {
     uint32_t k0, k1;
     int nchain, mc_steps, opt_steps, randomize;
@@ -307,32 +311,43 @@ __device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp,
 
 __device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
 
-__global__ void __launch_bounds__(256, 3) k_search(const int* __restrict__ blobs, const LigDev* __restrict__ ligs,
-                                                const int* __restrict__ order, int nlig, Env env, SearchP sp,
-                                                float* best, int* work_counter, unsigned long long* nevals) {
+// Work items are (ligand, first chain, chain count) in descending ligand cost; CTAs take
+// items from a global counter, re-stage the topology blob only when the ligand changes,
+// and their warps take the item's chains from a shared counter.  Large ligands are so
+// spread over many CTAs and the launch ends with the cheapest items.
+__global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __restrict__ blobs,
+                                                const LigDev* __restrict__ ligs, const int4* __restrict__ items,
+                                                int nitems, Env env, SearchP sp, float* best, int* work_counter,
+                                                unsigned long long* nevals) {
     extern __shared__ __align__(16) float smem[];
-    __shared__ int s_lig, s_next;
+    __shared__ int s_item, s_next, s_lig;
     int* sblob = reinterpret_cast<int*>(smem);
     float* wsbase = smem + sp.blob_max;
     const int warp = threadIdx.x >> 5, lane = lane_id();
     float* ws = wsbase + (size_t)warp * sp.ws_max;
     unsigned long long my_evals = 0, my_heavy = 0;
+    if (threadIdx.x == 0) s_lig = -1;
     while (true) {
-        if (threadIdx.x == 0) { s_lig = atomicAdd(work_counter, 1); s_next = 0; }
+        if (threadIdx.x == 0) { s_item = atomicAdd(work_counter, 1); s_next = 0; }
         __syncthreads();
-        int li = s_lig;
-        if (li >= nlig) break;
-        const LigDev L = ligs[order[li]];
-        for (int w = threadIdx.x; w < L.blob_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 item = items[it];          // (ligand, first chain, count, -)
+        const LigDev L = ligs[item.x];
+        if (item.x != s_lig) {
+            for (int w = threadIdx.x; w < L.blob_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+        }
         __syncthreads();
+        if (threadIdx.x == 0) s_lig = item.x;
         const Topo T = topo_view(sblob);
         const int nrec = 8 + 3 * T.natom + T.ntors;
         const Work W = work_at(ws, T.natom, T.ntors);
         while (true) {
-            int c = 0;
-            if (lane == 0) c = atomicAdd(&s_next, 1);
-            c = __shfl_sync(FULL, c, 0);
-            if (c >= sp.nchain) break;
+            int ci = 0;
+            if (lane == 0) ci = atomicAdd(&s_next, 1);
+            ci = __shfl_sync(FULL, ci, 0);
+            if (ci >= item.z) break;
+            const int c = item.y + ci;
             float* out = best + L.best_off + (long long)c * L.stride;
             Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
             int A = 0;
@@ -594,6 +609,7 @@ struct ud_ctx {
     long long best_floats = 0;
     DBuf<float> d_best;
     DBuf<int> d_order, d_counter, d_leaders, d_counts, d_sel, d_selcnt;
+    DBuf<int4> d_items;
     DBuf<unsigned long long> d_nevals;
     // results
     int num_pose = 0;
@@ -724,7 +740,7 @@ int ud_destroy(ud_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->d_rec.release(); c->d_maps32.release(); c->d_maps16.release();
     c->d_blobs.release(); c->d_ligs.release(); c->d_best.release();
-    c->d_order.release(); c->d_counter.release(); c->d_leaders.release(); c->d_counts.release();
+    c->d_order.release(); c->d_items.release(); c->d_counter.release(); c->d_leaders.release(); c->d_counts.release();
     c->d_sel.release(); c->d_selcnt.release(); c->d_nevals.release();
     c->d_out.release(); c->d_terms.release(); c->d_decomp.release();
     c->d_item_lig.release(); c->d_item_off.release(); c->d_item_off2.release();
@@ -1135,13 +1151,20 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
         tot += (long long)nchain * h.stride;
         wsm = std::max(wsm, ws_floats(h.natom, h.ntors));
         order[l] = l;
-        cost[l] = (double)(h.natom + 8) * (6 + h.ntors);   // rough: heavier ligands first
+        // evaluation cost ~ intra pairs + grid atoms + kinematics, times BFGS length
+        const double np = (double)(c->h_blobs[h.blob_off + H_NPAIR]);
+        cost[l] = (np + 8.0 * h.natom + 40.0 * h.ntors + 200.0) * (6 + h.ntors);
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<int4> items;
+    for (int l : order)
+        for (int c0 = 0; c0 < nchain; c0 += SEARCH_ITEM_CHAINS)
+            items.push_back(make_int4(l, c0, std::min(SEARCH_ITEM_CHAINS, nchain - c0), 0));
     upload_ligdev(c);
     c->best_floats = tot;
     c->d_best.ensure((size_t)tot);
-    c->d_order.upload(order.data(), nlig, c->stream);
+    c->d_items.upload(items.data(), items.size(), c->stream);
+    const int nitems = (int)items.size();
     c->d_counter.ensure(1);
     c->d_nevals.ensure(2);
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
@@ -1154,7 +1177,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     int per_sm = 0;
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, 32 * W, smem), "occupancy");
     if (per_sm < 1) per_sm = 1;
-    int grid = std::min(nlig, c->nsm * per_sm);
+    int grid = std::min(nitems, c->nsm * per_sm);
     SearchP sp;
     sp.k0 = (uint32_t)seed;
     sp.k1 = (uint32_t)(seed >> 32) ^ 0x5DEECE66u;
@@ -1165,7 +1188,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     sp.ws_max = wsm;
     sp.blob_max = blob_max;
     if (grid > 0) {
-        k_search<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_order.p, nlig, env, sp,
+        k_search<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, nitems, env, sp,
                                                     c->d_best.p, c->d_counter.p, c->d_nevals.p);
         ck(cudaGetLastError(), "k_search launch");
         c->counters[2]++;

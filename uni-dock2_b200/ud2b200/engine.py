@@ -32,7 +32,8 @@ _lib = None
 
 
 def lib_path() -> str:
-    return os.path.join(HERE, LIB_NAME)
+    """The engine library: UDOCK_B200_LIB if set, else the in-tree build."""
+    return os.environ.get("UDOCK_B200_LIB") or os.path.join(HERE, LIB_NAME)
 
 
 def load_library() -> C.CDLL:
