@@ -51,9 +51,20 @@ enum BlobHdr {
     H_RHOFF,       // T+1 ints: heavy rotated atoms per torsion
     H_RHEAVY,
     H_MAPIDX,      // natom ints: grid map slot of each atom (-1: none), set at upload
+    H_NPREC,       // number of heavy scored pairs (a count, not an offset)
+    H_PREC,        // 2 words per pair: i | j<<12 | hydrophobic<<24 | hbond<<25, and R_i + R_j (float)
+    H_AFLAGS,      // natom ints: heavy | hydrophobic<<1 | acceptor<<2 | donor<<3
+    H_PMASK,       // natom <= 32: one word per atom, bit b set if the heavy pair (a, b) is scored
+    H_GOFF,        // natom+1 ints: per-atom lists of (pair index, partner) for the gather
+    H_GADJ,        // entries: pair index | partner << 16
     H_TOTAL,
-    H_WORDS = 28
+    H_WORDS = 36
 };
+constexpr int AF_HEAVY = 1, AF_HYD = 2, AF_ACC = 4, AF_DON = 8;
+#ifndef RR32_MAX_ATOMS
+#define RR32_MAX_ATOMS 32      // ligands up to this size use the register round robin (<= 32)
+#endif
+constexpr int PREC_HYD = 1 << 24, PREC_HB = 1 << 25;
 constexpr int PAIR_ZERO = 1 << 16, PAIR_HYD = 1 << 17, PAIR_HB = 1 << 18;
 
 // Topology view: one base pointer and word offsets (keeps addressing 32-bit).
@@ -61,7 +72,7 @@ struct Topo {
     const int* b;
     int natom, ntors, nheavy, nbias;
     int o_types, o_axis, o_roff, o_ranges, o_rot_off, o_rot, o_pair_off, o_pairs, o_bias_off, o_bias, o_heavy,
-        o_radii, o_rhoff, o_rheavy, o_mapidx;
+        o_radii, o_rhoff, o_rheavy, o_mapidx, nprec, o_prec, o_aflags, o_pmask, o_goff, o_gadj;
     __device__ __forceinline__ int type(int i) const { return b[o_types + i]; }
     __device__ __forceinline__ int axis(int k) const { return b[o_axis + k]; }
     __device__ __forceinline__ int range_off(int k) const { return b[o_roff + k]; }
@@ -77,6 +88,11 @@ struct Topo {
     __device__ __forceinline__ int rh_off(int k) const { return b[o_rhoff + k]; }
     __device__ __forceinline__ int rheavy(int q) const { return b[o_rheavy + q]; }
     __device__ __forceinline__ int map_index(int i) const { return b[o_mapidx + i]; }
+    __device__ __forceinline__ int2 prec(int p) const { return *reinterpret_cast<const int2*>(b + o_prec + 2 * p); }
+    __device__ __forceinline__ int aflags(int i) const { return b[o_aflags + i]; }
+    __device__ __forceinline__ unsigned pmask(int i) const { return (unsigned)b[o_pmask + i]; }
+    __device__ __forceinline__ int goff(int i) const { return b[o_goff + i]; }
+    __device__ __forceinline__ int gadj(int k) const { return b[o_gadj + k]; }
 };
 
 __device__ __forceinline__ Topo topo_view(const int* b) {
@@ -101,6 +117,12 @@ __device__ __forceinline__ Topo topo_view(const int* b) {
     t.o_rhoff = b[H_RHOFF];
     t.o_rheavy = b[H_RHEAVY];
     t.o_mapidx = b[H_MAPIDX];
+    t.nprec = b[H_NPREC];
+    t.o_prec = b[H_PREC];
+    t.o_aflags = b[H_AFLAGS];
+    t.o_pmask = b[H_PMASK];
+    t.o_goff = b[H_GOFF];
+    t.o_gadj = b[H_GADJ];
     return t;
 }
 
@@ -176,6 +198,33 @@ __device__ __forceinline__ float vina_ef(float d, bool hyd, bool hb, float& f) {
     return e;
 }
 
+// Intra pair term seen from atom a of the pair (a, b), d = x_b - x_a: returns the pair
+// energy after the per-pair curl and the scalar s with force on a = -s d.  The reaction
+// on b is the negation, bit for bit what the reference computes from b's side (the
+// squared distance, radius sum and Vina terms are symmetric).
+__device__ __forceinline__ float pair_scalar(float dx, float dy, float dz, float rsum, bool hyd, bool hb, float vcap,
+                                             float& s_out) {
+    s_out = 0.f;
+    const float rr = dx * dx + dy * dy + dz * dz;
+    if (!(rr < 64.f)) return 0.f;
+    const float rsq = rsqrtf(rr);                       // r and 1/r from one reciprocal root;
+    const float rn = rr > 0.f ? rr * rsq : 0.f;         // r is clamped at EPSILON before dividing
+    float fdr;
+    float ep = vina_ef(rn - rsum, hyd, hb, fdr);
+    fdr *= rn < EPS_F ? (1.f / EPS_F) : rsq;
+    if (ep > 0.f) {
+        const float c = __fdividef(vcap, vcap + ep);
+        ep *= c;
+        fdr *= c * c;
+    }
+    s_out = fdr;
+    return ep;
+}
+__device__ __forceinline__ bool flags_hyd(int fa, int fb) { return (fa & fb & AF_HYD) != 0; }
+__device__ __forceinline__ bool flags_hb(int fa, int fb) {
+    return ((fa & AF_ACC) && (fb & AF_DON)) || ((fa & AF_DON) && (fb & AF_ACC));
+}
+
 __device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
     f = 0.f;
     if (t1 == VN_H || t2 == VN_H) return 0.f;
@@ -241,14 +290,23 @@ struct Rng {
 };
 
 // ---------------------------------------------------------------- small math
+// fmodf(x, 2 PI) with exact shortcuts for the common magnitudes: |x| < 2 PI is returned
+// unchanged and 2 PI <= |x| < 4 PI loses one period, both exactly what fmodf returns
+// (the subtraction is exact by Sterbenz's lemma)
+__device__ __forceinline__ float fmod_2pi(float x) {
+    const float p = 2.f * PI_F, ax = fabsf(x);
+    if (ax < p) return x;
+    if (ax < 2.f * p) return x > 0.f ? x - p : x + p;
+    return fmodf(x, p);
+}
 __device__ __forceinline__ float normalize_angle(float x) {   // mymath.h:38-47
-    x = fmodf(x, 2.f * PI_F);
+    x = fmod_2pi(x);
     if (x < -PI_F) x += 2.f * PI_F;
     if (x > PI_F) x -= 2.f * PI_F;
     return x;
 }
 __device__ __forceinline__ float normalize_angle_2pi(float x) {
-    x = fmodf(x, 2.f * PI_F);
+    x = fmod_2pi(x);
     if (x < 0.f) x += 2.f * PI_F;
     return x;
 }
@@ -269,10 +327,11 @@ __device__ __forceinline__ void rotvec_to_quat(float vx, float vy, float vz, flo
     if (th > EPS_F) {
         float s, c;
         sincosf(th * 0.5f, &s, &c);
+        const float k = __fdividef(s, th);
         q0 = c;
-        q1 = s * (vx / th);
-        q2 = s * (vy / th);
-        q3 = s * (vz / th);
+        q1 = k * vx;
+        q2 = k * vy;
+        q3 = k * vz;
     } else {
         q0 = 1.f; q1 = q2 = q3 = 0.f;
     }
@@ -409,10 +468,104 @@ __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x
     return e;
 }
 
+// ---------------------------------------------------------------- intra pairs
+// The reference visits every scored pair from both atoms (per-pair curl, energy halved,
+// bfgs.cuh:305-352).  Both visits give the same energy and opposite forces, so each
+// heavy pair is evaluated once here.  The functions add the intra forces to F (which
+// holds the inter forces of the lane's own atoms) and return the lane's share of the
+// intra energy.  The kernel is issue bound, so each variant keeps the number of
+// evaluated pair slots close to the number of pairs.
+
+// natom <= 32: a round robin in registers.  Lane a owns atom a; in round t = 1..16 it
+// pairs with atom (a + t) mod 32, fetched by shuffle (at t = 16 only a < 16 computes),
+// keeps the force on its own atom and hands the reaction back by shuffle.  Every pair is
+// visited once; no shared memory, no atomics, fixed summation order.
+__device__ __forceinline__ float intra_rr32(const Topo& T, const float* X, float* F, float vcap) {
+    const int a = lane_id();
+    const bool va = a < T.natom;
+    float xa = 0.f, ya = 0.f, za = 0.f, Ra = 0.f;
+    int fa = 0;
+    unsigned ma = 0u;
+    if (va) {
+        xa = X[3 * a]; ya = X[3 * a + 1]; za = X[3 * a + 2];
+        Ra = T.radius(a); fa = T.aflags(a); ma = T.pmask(a);
+    }
+    float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
+#pragma unroll 1
+    for (int t = 1; t <= 16; t++) {
+        const int b = (a + t) & 31;
+        const float xb = __shfl_sync(FULL, xa, b), yb = __shfl_sync(FULL, ya, b), zb = __shfl_sync(FULL, za, b);
+        const float Rb = __shfl_sync(FULL, Ra, b);
+        const int fb = __shfl_sync(FULL, fa, b);
+        const float dx = xb - xa, dy = yb - ya, dz = zb - za;
+        float sc = 0.f;
+        if (((ma >> b) & 1u) && (t < 16 || a < 16))
+            e += pair_scalar(dx, dy, dz, Ra + Rb, flags_hyd(fa, fb), flags_hb(fa, fb), vcap, sc);
+        const float px = -sc * dx, py = -sc * dy, pz = -sc * dz;       // force on a
+        const int src = (a - t) & 31;                                  // the lane that paired with a
+        fx += px - __shfl_sync(FULL, px, src);
+        fy += py - __shfl_sync(FULL, py, src);
+        fz += pz - __shfl_sync(FULL, pz, src);
+    }
+    if (va) { F[3 * a] += fx; F[3 * a + 1] += fy; F[3 * a + 2] += fz; }
+    return e;
+}
+
+// more than 32 atoms: pass 1 evaluates every pair once, pairs spread evenly over the
+// lanes, and stores the force scalar of each pair in the warp's pair buffer PB; pass 2
+// gathers F_a += s_p (x_a - x_b) over the atom's pairs in pair-index order
+__device__ __forceinline__ float intra_buffered(const Topo& T, const float* X, float* F, float vcap, float* PB) {
+    const int lane = lane_id();
+    float e = 0.f;
+    for (int p = lane; p < T.nprec; p += WARP) {
+        const int2 pr = T.prec(p);
+        const int i = pr.x & 0xFFF, j = (pr.x >> 12) & 0xFFF;
+        float sc;
+        e += pair_scalar(X[3 * j] - X[3 * i], X[3 * j + 1] - X[3 * i + 1], X[3 * j + 2] - X[3 * i + 2],
+                         __int_as_float(pr.y), pr.x & PREC_HYD, pr.x & PREC_HB, vcap, sc);
+        PB[p] = sc;
+    }
+    __syncwarp();
+    for (int a = lane; a < T.natom; a += WARP) {
+        const float xa = X[3 * a], ya = X[3 * a + 1], za = X[3 * a + 2];
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        const int k1 = T.goff(a + 1);
+        for (int k = T.goff(a); k < k1; k++) {
+            const int ent = T.gadj(k);
+            const float sc = PB[ent & 0xFFFF];
+            const int b = ent >> 16;
+            fx += sc * (xa - X[3 * b]);
+            fy += sc * (ya - X[3 * b + 1]);
+            fz += sc * (za - X[3 * b + 2]);
+        }
+        F[3 * a] += fx; F[3 * a + 1] += fy; F[3 * a + 2] += fz;
+    }
+    return e;
+}
+
+// ligands whose pair list does not fit the pair buffer: pairs spread over the lanes,
+// forces accumulated with shared-memory atomic adds
+__device__ __forceinline__ float intra_atomic(const Topo& T, const float* X, float* F, float vcap) {
+    float e = 0.f;
+    for (int p = lane_id(); p < T.nprec; p += WARP) {
+        const int2 pr = T.prec(p);
+        const int i = pr.x & 0xFFF, j = (pr.x >> 12) & 0xFFF;
+        const float dx = X[3 * j] - X[3 * i], dy = X[3 * j + 1] - X[3 * i + 1], dz = X[3 * j + 2] - X[3 * i + 2];
+        float sc;
+        e += pair_scalar(dx, dy, dz, __int_as_float(pr.y), pr.x & PREC_HYD, pr.x & PREC_HB, vcap, sc);
+        if (sc != 0.f) {
+            atomicAdd(F + 3 * i, -sc * dx); atomicAdd(F + 3 * i + 1, -sc * dy); atomicAdd(F + 3 * i + 2, -sc * dz);
+            atomicAdd(F + 3 * j, sc * dx); atomicAdd(F + 3 * j + 1, sc * dy); atomicAdd(F + 3 * j + 2, sc * dz);
+        }
+    }
+    return e;
+}
+
 // ---------------------------------------------------------------- energy + force
 // Fills F (3N, dE/dx per atom) and returns the warp-summed energy (bfgs.cuh:221-394).
+// PB: the warp's pair buffer for ligands above 32 atoms (null: atomic accumulation).
 __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* F, float vcap,
-                                          float slope) {
+                                          float slope, float* PB) {
     const int lane = lane_id();
     float energy = 0.f;
     // inter + penalty
@@ -460,40 +613,9 @@ __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const f
         F[3 * i] = fx; F[3 * i + 1] = fy; F[3 * i + 2] = fz;
     }
     __syncwarp();
-    // intra (bfgs.cuh:305-352): per-atom adjacency in both directions, per-pair curl;
-    // entries carry the pair flags, hydrogen pairs are marked and contribute nothing
-    float e_intra = 0.f;
-    for (int i = lane; i < T.natom; i += WARP) {
-        const float r1 = T.radius(i);
-        const float xi = X[3 * i], yi = X[3 * i + 1], zi = X[3 * i + 2];
-        float fx = 0.f, fy = 0.f, fz = 0.f, ea = 0.f;
-        const int k1 = T.pair_off(i + 1);
-        for (int k = T.pair_off(i); k < k1; k++) {
-            const int ent = T.pair(k);
-            if (ent & PAIR_ZERO) continue;
-            const int j = ent & 0xFFFF;
-            const float rv0 = X[3 * j] - xi, rv1 = X[3 * j + 1] - yi, rv2 = X[3 * j + 2] - zi;
-            const float rr = rv0 * rv0 + rv1 * rv1 + rv2 * rv2;
-            if (rr < 64.f) {
-                float rn = sqrtf(rr), fdr;
-                float ep = vina_ef(rn - (r1 + T.radius(j)), ent & PAIR_HYD, ent & PAIR_HB, fdr);
-                if (rn < EPS_F) rn = EPS_F;
-                fdr /= rn;
-                float px = -fdr * rv0, py = -fdr * rv1, pz = -fdr * rv2;
-                if (ep > 0.f) {
-                    float s = vcap / (vcap + ep);
-                    ep *= s;
-                    s *= s;
-                    px *= s; py *= s; pz *= s;
-                }
-                ea += ep;
-                fx += px; fy += py; fz += pz;
-            }
-        }
-        e_intra += ea;
-        F[3 * i] += fx; F[3 * i + 1] += fy; F[3 * i + 2] += fz;
-    }
-    energy += 0.5f * e_intra;
+    if (T.natom <= RR32_MAX_ATOMS) energy += intra_rr32(T, X, F, vcap);
+    else if (PB) energy += intra_buffered(T, X, F, vcap, PB);
+    else energy += intra_atomic(T, X, F, vcap);
     // bias (bfgs.cuh:356-388; vina.h:353-400)
     if (env.bias_type != 0 && T.nbias > 0) {
         __syncwarp();
@@ -586,8 +708,8 @@ __device__ __forceinline__ void grad_from_forces(const Topo& T, const Env& env, 
 }
 
 __device__ __forceinline__ float eval_e_grad(const Topo& T, const Env& env, Slot P, float* F, float* G,
-                                             float vcap, float slope) {
-    float e = eval_e_f(T, env, P.x, F, vcap, slope);
+                                             float vcap, float slope, float* PB) {
+    float e = eval_e_f(T, env, P.x, F, vcap, slope, PB);
     grad_from_forces(T, env, P, F, G);
     return e;
 }
@@ -648,7 +770,7 @@ __device__ __forceinline__ void apply_dihe(const Topo& T, Slot P, int k, float i
     applied = __shfl_sync(FULL, applied, 0);
     __syncwarp();
     float s, c;
-    sincosf(applied, &s, &c);
+    __sincosf(applied, &s, &c);
     rotate_torsion(T, P, k, s, c);
     refresh_center(T, P);
 }
@@ -663,7 +785,7 @@ __device__ __forceinline__ void apply_update(const Topo& T, const Env& env, Slot
     for (int k = lane; k < T.ntors; k += WARP) {
         const float applied = dihedral_step(T, P, k, G[6 + k] * alpha);
         float s, c;
-        sincosf(applied, &s, &c);
+        __sincosf(applied, &s, &c);       // |applied| <= 2 pi: hardware sine/cosine (~1e-6 abs)
         SC[2 * k] = s;
         SC[2 * k + 1] = c;
     }
@@ -699,6 +821,7 @@ struct Work {        // per-warp scratch in shared memory
     float* mhy;      // D
     float* sc;       // 2T torsion sine/cosine scratch
     double* H;       // D(D+1)/2, packed upper triangle: H[i + j(j+1)/2], i <= j
+    float* pb;       // pair buffer for ligands above 32 atoms, or null
 };
 
 __device__ __forceinline__ float gdot(const float* a, const float* b, int n) {
@@ -728,7 +851,7 @@ __device__ __forceinline__ float line_search(const Topo& T, const Env& env, Slot
     for (int trial = 0; trial < LS_STEPS; trial++) {
         slot_copy(Pn, Px, T.natom, T.ntors);
         apply_update(T, env, Pn, W.p, alpha, W.sc);
-        e_new = eval_e_grad(T, env, Pn, W.F, W.gn, vcap, slope);
+        e_new = eval_e_grad(T, env, Pn, W.F, W.gn, vcap, slope, W.pb);
         n_eval++;
         if (e_new - e0 < 1e-4f * alpha * pg) break;
         alpha *= 0.5f;
@@ -744,7 +867,7 @@ __device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots,
     const int lane = lane_id();
     const int dim = 6 + T.ntors;
     const Slot X = slot_at(slots, stride, ix, T.natom);
-    const float E_ori = eval_e_grad(T, env, X, W.F, W.g, vcap, slope);
+    const float E_ori = eval_e_grad(T, env, X, W.F, W.g, vcap, slope, W.pb);
     n_eval++;
     float E = E_ori;
     const int ntri = dim * (dim + 1) / 2;

@@ -31,9 +31,20 @@ static const float kVdwHost[NT] = {1.1f, 1.92f, 1.9f, 1.9f, 1.8f, 1.8f, 1.8f, 1.
 // ====================================================================== layout helpers
 __host__ __device__ inline int r4(int x) { return (x + 3) & ~3; }
 __host__ __device__ inline int rec_floats(int n, int t) { return r4(8 + 3 * n + t); }
-__host__ __device__ inline int ws_floats(int n, int t) {
+// pair buffer floats of a ligand: used above 32 atoms while the pair list fits PB_MAX
+#ifndef PB_MAX_FLOATS
+#define PB_MAX_FLOATS 4096
+#endif
+#ifndef PB_MIN_ATOMS
+#define PB_MIN_ATOMS RR32_MAX_ATOMS
+#endif
+constexpr int PB_MAX = PB_MAX_FLOATS;
+__host__ __device__ inline int pb_floats(int n, int npair) {
+    return (n > PB_MIN_ATOMS && npair <= PB_MAX) ? r4(npair) : 0;
+}
+__host__ __device__ inline int ws_floats(int n, int t, int npair) {
     int d = 6 + t;
-    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(2 * t) + r4(d * (d + 1));
+    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(2 * t) + r4(d * (d + 1)) + pb_floats(n, npair);
 }
 
 struct LigDev {
@@ -47,8 +58,8 @@ struct LigDev {
     long long out_off;   // float offset of the output records (num_pose capacity)
 };
 
-__device__ __forceinline__ Work work_at(float* ws, int natom, int ntors) {
-    int d = 6 + ntors;
+__device__ __forceinline__ Work work_at(float* ws, const Topo& T) {
+    const int natom = T.natom, ntors = T.ntors, d = 6 + ntors;
     Work W;
     W.F = ws + 4 * rec_floats(natom, ntors);
     W.g = W.F + r4(3 * natom);
@@ -58,6 +69,7 @@ __device__ __forceinline__ Work work_at(float* ws, int natom, int ntors) {
     W.mhy = W.y + r4(d);
     W.sc = W.mhy + r4(d);
     W.H = reinterpret_cast<double*>(W.sc + r4(2 * ntors));
+    W.pb = pb_floats(natom, T.nprec) ? reinterpret_cast<float*>(W.H) + r4(d * (d + 1)) : nullptr;
     return W;
 }
 
@@ -159,12 +171,12 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
     const int* blob = blobs + L.blob_off;
     Topo T = topo_view(blob);
     Slot P = slot_at(ws, L.stride, 0, T.natom);
-    Work W = work_at(ws, T.natom, T.ntors);
+    Work W = work_at(ws, T);
     const float* x = io.xyz + io.xoff[pose];
     for (int i = lane; i < 3 * T.natom; i += WARP) P.x[i] = x[i];
     if (lane < 3) { P.h[1 + lane] = io.centers[3 * pose + lane]; P.h[4 + lane] = io.rotvecs[3 * pose + lane]; }
     __syncwarp();
-    float e = eval_e_grad(T, env, P, W.F, W.g, vcap, slope);
+    float e = eval_e_grad(T, env, P, W.F, W.g, vcap, slope, W.pb);
     if (lane == 0) out_e[pose] = e;
     float* g = out_g + io.goff[pose];
     for (int i = lane; i < 6 + T.ntors; i += WARP) g[i] = W.g[i];
@@ -276,7 +288,7 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
     float* ws = smem + (size_t)warp * ws_max;
     const LigDev L = ligs[item_lig[item]];
     Topo T = topo_view(blobs + L.blob_off);
-    Work W = work_at(ws, T.natom, T.ntors);
+    Work W = work_at(ws, T);
     float* rec = recs + item_off[item];
     int nrec = 8 + 3 * T.natom + T.ntors;
     copy_words(ws, rec, nrec);
@@ -341,7 +353,7 @@ __global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __
         if (threadIdx.x == 0) s_lig = item.x;
         const Topo T = topo_view(sblob);
         const int nrec = 8 + 3 * T.natom + T.ntors;
-        const Work W = work_at(ws, T.natom, T.ntors);
+        const Work W = work_at(ws, T);
         while (true) {
             int ci = 0;
             if (lane == 0) ci = atomicAdd(&s_next, 1);
@@ -357,7 +369,7 @@ __global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __
             int ne = 0;
             float best_e = 1e9f;
             if (sp.mc_steps == 0) {
-                float e = eval_e_f(T, env, SA.x, W.F, VCAP_SEARCH, PENALTY_SLOPE);
+                float e = eval_e_f(T, env, SA.x, W.F, VCAP_SEARCH, PENALTY_SLOPE, W.pb);
                 ne++;
                 if (lane == 0) SA.h[0] = e;
                 __syncwarp();
@@ -374,7 +386,7 @@ __global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __
                     const float e_acc = ws[A * L.stride];
                     const float rx = u01(rng.draw((uint32_t)step, P_METRO).x);
                     if (sp.opt_steps == 0) {
-                        float e = eval_e_grad(T, env, SC, W.F, W.g, VCAP_SEARCH, PENALTY_SLOPE);
+                        float e = eval_e_grad(T, env, SC, W.F, W.g, VCAP_SEARCH, PENALTY_SLOPE, W.pb);
                         ne++;
                         if (lane == 0) SC.h[0] = e;
                         __syncwarp();
@@ -575,9 +587,10 @@ struct DBuf {
 };
 
 struct LigHost {
-    int natom, ntors, nheavy, blob_words, stride;
+    int natom, ntors, nheavy, blob_words, stride, nprec;
     long long blob_off;
 };
+inline int lig_ws(const LigHost& h) { return ws_floats(h.natom, h.ntors, h.nprec); }
 }  // namespace
 
 struct ud_ctx {
@@ -953,12 +966,73 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
             }
             o = put(H_MAPIDX, n);      // filled from the current grid at upload (sync_ligs)
             for (int i = 0; i < n; i++) blob[o + i] = -1;
+            {   // heavy scored pairs, once each (i < j), for the intra kernels, in round-robin
+                // order (pair (a, a+t mod n) for t = 1..n/2) so that 32 consecutive pairs touch
+                // each atom about twice
+                std::vector<char> scored((size_t)n * n, 0);
+                for (int i = 0; i < n; i++)
+                    for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++)
+                        scored[(size_t)i * n + pairs[p0 + k]] = 1;
+                std::vector<int> rec;
+                for (int t = 1; t <= n / 2; t++)
+                    for (int a = 0; a < n; a++) {
+                        if (2 * t == n && a >= t) break;
+                        const int i = std::min(a, (a + t) % n), j = std::max(a, (a + t) % n);
+                        if (!scored[(size_t)i * n + j] && !scored[(size_t)j * n + i]) continue;
+                        const int ti = types[a0 + i], tj = types[a0 + j];
+                        if (ti == VN_H || tj == VN_H) continue;
+                        const unsigned b1 = 1u << ti, b2 = 1u << tj;
+                        int w0 = i | (j << 12);
+                        if ((b1 & HYD_MASK) && (b2 & HYD_MASK)) w0 |= PREC_HYD;
+                        if (((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK))) w0 |= PREC_HB;
+                        const float rs = kVdwHost[ti] + kVdwHost[tj];
+                        int w1;
+                        memcpy(&w1, &rs, sizeof(w1));
+                        rec.push_back(w0);
+                        rec.push_back(w1);
+                    }
+                const int np2 = (int)rec.size() / 2;
+                if (np2 > 0xFFFF) throw Fail(UD_EINVAL, "too many intra pairs (max 65535)");
+                blob[H_NPREC] = np2;
+                o = put(H_PREC, (int)rec.size());
+                for (size_t q = 0; q < rec.size(); q++) blob[o + q] = rec[q];
+                o = put(H_AFLAGS, n);
+                for (int i = 0; i < n; i++) {
+                    const int t = types[a0 + i];
+                    const unsigned b = 1u << t;
+                    blob[o + i] = (t != VN_H ? AF_HEAVY : 0) | ((b & HYD_MASK) ? AF_HYD : 0) |
+                                  ((b & ACC_MASK) ? AF_ACC : 0) | ((b & DON_MASK) ? AF_DON : 0);
+                }
+                // partner masks for the register round robin (ligands of at most 32 atoms)
+                o = put(H_PMASK, n <= 32 ? n : 0);
+                if (n <= 32)
+                    for (int p = 0; p < np2; p++) {
+                        const int i = rec[2 * p] & 0xFFF, j = (rec[2 * p] >> 12) & 0xFFF;
+                        blob[o + i] |= (int)(1u << j);
+                        blob[o + j] |= (int)(1u << i);
+                    }
+                // gather lists: for each atom, (pair index, partner) in pair-index order
+                std::vector<std::vector<int>> g(n);
+                for (int p = 0; p < np2; p++) {
+                    const int i = rec[2 * p] & 0xFFF, j = (rec[2 * p] >> 12) & 0xFFF;
+                    g[i].push_back(p | (j << 16));
+                    g[j].push_back(p | (i << 16));
+                }
+                o = put(H_GOFF, n + 1);
+                int acc = 0;
+                for (int i = 0; i < n; i++) { blob[o + i] = acc; acc += (int)g[i].size(); }
+                blob[o + n] = acc;
+                o = put(H_GADJ, acc);
+                for (int i = 0, k = 0; i < n; i++)
+                    for (int v : g[i]) blob[o + k++] = v;
+            }
             blob[H_TOTAL] = (int)blob.size();
             LigHost h;
             h.natom = n; h.ntors = T; h.nheavy = nheavy;
             h.blob_words = (int)blob.size();
             h.blob_off = (long long)c->h_blobs.size();
             h.stride = rec_floats(n, T);
+            h.nprec = blob[H_NPREC];
             c->h_blobs.insert(c->h_blobs.end(), blob.begin(), blob.end());
             c->h_ligs.push_back(h);
             c->max_natom = std::max(c->max_natom, n);
@@ -1011,7 +1085,7 @@ int ud_score_batch(ud_ctx* c, int n, const int* pose_lig, const float* coords, c
             goff[i] = gs;
             xs += 3LL * c->h_ligs[l].natom;
             gs += 6 + c->h_ligs[l].ntors;
-            wsm = std::max(wsm, ws_floats(c->h_ligs[l].natom, c->h_ligs[l].ntors));
+            wsm = std::max(wsm, lig_ws(c->h_ligs[l]));
         }
         DBuf<int> dl; DBuf<long long> dxo, dgo; DBuf<float> dx, dc, dr, de, dg;
         dl.upload(pose_lig, n, c->stream);
@@ -1097,7 +1171,7 @@ int ud_bfgs_batch(ud_ctx* c, int n, const int* pose_lig, float* records, int max
             if (l < 0 || l >= (int)c->h_ligs.size()) throw Fail(UD_EINVAL, "pose ligand index out of range");
             off[i] = tot;
             tot += c->h_ligs[l].stride;
-            wsm = std::max(wsm, ws_floats(c->h_ligs[l].natom, c->h_ligs[l].ntors));
+            wsm = std::max(wsm, lig_ws(c->h_ligs[l]));
         }
         // records are packed at 8+3N+T floats each on the host side
         std::vector<float> packed(tot, 0.f);
@@ -1149,7 +1223,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
         const LigHost& h = c->h_ligs[l];
         c->h_ligdev[l].best_off = tot;
         tot += (long long)nchain * h.stride;
-        wsm = std::max(wsm, ws_floats(h.natom, h.ntors));
+        wsm = std::max(wsm, lig_ws(h));
         order[l] = l;
         // evaluation cost ~ intra pairs + grid atoms + kinematics, times BFGS length
         const double np = (double)(c->h_blobs[h.blob_off + H_NPAIR]);
@@ -1295,7 +1369,7 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
             int wsm = 0;
             for (int l = 0; l < nlig; l++) {
                 const LigHost& h = c->h_ligs[l];
-                wsm = std::max(wsm, ws_floats(h.natom, h.ntors));
+                wsm = std::max(wsm, lig_ws(h));
                 for (int k = 0; k < counts[l]; k++) {
                     il.push_back(l);
                     io.push_back(c->h_ligdev[l].best_off + (long long)leaders[(size_t)l * p->nchain + k] * h.stride);
