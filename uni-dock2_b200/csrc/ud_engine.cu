@@ -5,8 +5,8 @@
 //   k_score        E + generalised gradient of a pose batch   (src/cuda/bfgs_wrapper.cu:51-98)
 //   k_terms        final score terms, no curl                 (src/score/score.cpp:12-147)
 //   k_bfgs         BFGS / refinement rounds on pose records   (src/cuda/optimize.cu:14-77)
-//   k_search       persistent MC search: CTA per ligand, warp per chain, chains of a
-//                  ligand handed out from a shared counter    (src/cuda/mc.cu:109-448)
+//   k_search       persistent MC search: warp per chain; CTAs take (ligand, chain block)
+//                  work items in cost order from a global counter (src/cuda/mc.cu:109-448)
 //   k_cluster      CTA per ligand: energy ranking + greedy RMSD leaders (src/cuda/cluster.cu)
 //   k_filter       CTA per ligand: energy_range / num_pose filter (src/task/DockTask.cpp:188-220)
 // Host orchestration replaces DockTask::run (src/task/DockTask.cpp:39-123).
@@ -308,7 +308,6 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
 #ifndef SEARCH_MIN_BLOCKS
 #define SEARCH_MIN_BLOCKS 4          // 256-thread CTAs per SM the register budget is sized for
 #endif
-constexpr int SEARCH_ITEM_CHAINS = 16;
 struct SearchP {
     uint32_t k0, k1;
     int nchain, mc_steps, opt_steps, randomize;
@@ -323,10 +322,10 @@ __device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp,
 
 __device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
 
-// Work items are (ligand, first chain, chain count) in descending ligand cost; CTAs take
-// items from a global counter, re-stage the topology blob only when the ligand changes,
-// and their warps take the item's chains from a shared counter.  Large ligands are so
-// spread over many CTAs and the launch ends with the cheapest items.
+// Work items are (ligand, first chain, chain count <= warps per CTA) in descending ligand
+// cost; CTAs take items from a global counter, re-stage the topology blob only when the
+// ligand changes, and their warps take the item's chains from a shared counter.  Large
+// ligands are so spread over many CTAs and the launch ends with the cheapest items.
 __global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __restrict__ blobs,
                                                 const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                 int nitems, Env env, SearchP sp, float* best, int* work_counter,
@@ -1230,10 +1229,15 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
         cost[l] = (np + 8.0 * h.natom + 40.0 * h.ntors + 200.0) * (6 + h.ntors);
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    int blob_max = r4(c->max_blob);
+    int W = pick_warps(c, wsm, blob_max, 8);
+    size_t smem = ((size_t)blob_max + (size_t)W * wsm) * 4;
+    // one chain per warp per item: a CTA finishes an item in one chain time, so small
+    // batches still fill every resident CTA and the tail is one chain long
     std::vector<int4> items;
     for (int l : order)
-        for (int c0 = 0; c0 < nchain; c0 += SEARCH_ITEM_CHAINS)
-            items.push_back(make_int4(l, c0, std::min(SEARCH_ITEM_CHAINS, nchain - c0), 0));
+        for (int c0 = 0; c0 < nchain; c0 += W)
+            items.push_back(make_int4(l, c0, std::min(W, nchain - c0), 0));
     upload_ligdev(c);
     c->best_floats = tot;
     c->d_best.ensure((size_t)tot);
@@ -1244,9 +1248,6 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
     ck(cudaMemsetAsync(c->d_nevals.p, 0, 2 * sizeof(unsigned long long), c->stream), "memset");
     c->counters[3] = (long long)nlig * nchain;
-    int blob_max = r4(c->max_blob);
-    int W = pick_warps(c, wsm, blob_max, 8);
-    size_t smem = ((size_t)blob_max + (size_t)W * wsm) * 4;
     set_smem(k_search, smem);
     int per_sm = 0;
     ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, 32 * W, smem), "occupancy");
