@@ -107,6 +107,28 @@ int ud_ligand_count(const ud_ctx* ctx);
 int ud_score_batch(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, const float* centers,
                    const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g);
 
+/* ud_score_batch without any device-memory allocation.  No counterpart in the reference.
+ * For callers that must not allocate device memory inside the call: a host whose device
+ * memory is already handed to its own pool allocator, or a loop that cannot afford the
+ * device-wide synchronisation that cudaFree implies.  Same arguments, results and errors
+ * as ud_score_batch; the per-call staging lives in one fixed module-scope device array
+ * of UD_NOALLOC_SCRATCH_BYTES per device instead of fresh buffers.
+ * - Limits: n <= UD_NOALLOC_MAX_POSES, and the batch's staging (ids, 2 int64 offsets,
+ *   coordinates, centres, rotation vectors, energies, gradients; each 256-byte aligned)
+ *   must fit UD_NOALLOC_SCRATCH_BYTES; larger batches fail with UD_EINVAL: split them.
+ * - The ligand set must already be on the device: after ud_add_ligands / ud_build_grid,
+ *   one ud_score_batch, ud_search or ud_dock call uploads it; otherwise UD_ESTATE.
+ * - First call on a device: looks the array's address up (cudaGetSymbolAddress) with
+ *   that device current, once; make this first call before any stream capture begins.
+ * - Nothing in the array has to start at zero: every word a call reads it wrote first.
+ * - All contexts on a device share the one array: calls that overlap in time (from
+ *   several threads, or several contexts on one device) race on it and must be
+ *   serialised by the caller. */
+#define UD_NOALLOC_MAX_POSES 16384
+#define UD_NOALLOC_SCRATCH_BYTES (8u << 20)
+int ud_score_batch_noalloc(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, const float* centers,
+                           const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g);
+
 /* Final-score terms of n poses without curl: out_terms4 = [intra(i<j), inter, penalty, bias]
  * per pose; out_decomp (nullable) = 5 inter terms per atom
  * [gauss1, gauss2, repulsion, hydrophobic, hbond].

@@ -19,6 +19,7 @@
 #include <vector>
 #include <algorithm>
 #include <stdexcept>
+#include <mutex>
 #include "ud_device.cuh"
 #include "../../include/udock_b200.h"
 
@@ -180,6 +181,65 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
     if (lane == 0) out_e[pose] = e;
     float* g = out_g + io.goff[pose];
     for (int i = lane; i < 6 + T.ntors; i += WARP) g[i] = W.g[i];
+}
+
+// ---------------------------------------------------------------------- no-allocation scoring
+// Staging area of ud_score_batch_noalloc: one per device (module-scope, allocated when the
+// module loads), shared by every context on that device.  Holds, 256-byte aligned in
+// this order: pose ligand ids (int), coordinate and gradient offsets (int64), coordinates,
+// centres, rotation vectors, energies and gradients (float).
+#ifndef UD_NOALLOC_SCRATCH_BYTES
+#define UD_NOALLOC_SCRATCH_BYTES (8u << 20)
+#endif
+static __device__ __align__(256) unsigned char g_noalloc_scratch[UD_NOALLOC_SCRATCH_BYTES];
+
+// exclusive prefix sums of 3*natom and 6+ntors over the poses (one CTA of 1024 threads)
+__global__ void __launch_bounds__(1024) k_pose_offsets(const LigDev* __restrict__ ligs, int n,
+                                                       const int* __restrict__ pose_lig, long long* xoff,
+                                                       long long* goff) {
+    __shared__ long long sx[32], sg[32];
+    __shared__ long long carry_x, carry_g;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    if (threadIdx.x == 0) { carry_x = 0; carry_g = 0; }
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        long long vx = 0, vg = 0;
+        if (i < n) {
+            const LigDev L = ligs[pose_lig[i]];
+            vx = 3LL * L.natom;
+            vg = 6LL + L.ntors;
+        }
+        long long ix = vx, ig = vg;          // inclusive warp scan
+        for (int d = 1; d < WARP; d <<= 1) {
+            long long tx = __shfl_up_sync(FULL, ix, d), tg = __shfl_up_sync(FULL, ig, d);
+            if (lane >= d) { ix += tx; ig += tg; }
+        }
+        if (lane == WARP - 1) { sx[warp] = ix; sg[warp] = ig; }
+        __syncthreads();
+        if (warp == 0) {                     // scan of the warp totals
+            long long wx = lane < (int)(blockDim.x >> 5) ? sx[lane] : 0;
+            long long wg = lane < (int)(blockDim.x >> 5) ? sg[lane] : 0;
+            for (int d = 1; d < WARP; d <<= 1) {
+                long long tx = __shfl_up_sync(FULL, wx, d), tg = __shfl_up_sync(FULL, wg, d);
+                if (lane >= d) { wx += tx; wg += tg; }
+            }
+            sx[lane] = wx;
+            sg[lane] = wg;
+        }
+        __syncthreads();
+        const long long px = (warp ? sx[warp - 1] : 0) + carry_x, pg = (warp ? sg[warp - 1] : 0) + carry_g;
+        if (i < n) {
+            xoff[i] = px + ix - vx;
+            goff[i] = pg + ig - vg;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) {
+            carry_x = px + ix;
+            carry_g = pg + ig;
+        }
+        __syncthreads();
+    }
 }
 
 // score() without curl: intra over i<j, inter, penalty (slope 1e6), bias (score.cpp:12-108);
@@ -1526,3 +1586,94 @@ int ud_sync(ud_ctx* c) {
 }
 
 }  // extern "C"
+
+// ====================================================================== no-allocation scoring
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// device address of g_noalloc_scratch on `device` (which must be current), looked up once
+unsigned char* noalloc_scratch(int device) {
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) throw Fail(UD_EINVAL, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        ck(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress (no-allocation scratch)");
+        g_noalloc_ptr[device] = p;
+    }
+    return static_cast<unsigned char*>(g_noalloc_ptr[device]);
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+}  // namespace
+
+extern "C" int ud_score_batch_noalloc(ud_ctx* c, int n, const int* pose_lig, const float* coords,
+                                      const float* centers, const float* rotvecs, int mode, float vcap, float slope,
+                                      float* out_e, float* out_g) {
+    try {
+        if (!c || n < 0 || (n > 0 && (!pose_lig || !coords || !centers || !rotvecs || !out_e || !out_g)))
+            throw Fail(UD_EINVAL, "invalid score arguments");
+        if (n == 0) return UD_OK;
+        if (n > UD_NOALLOC_MAX_POSES)
+            throw Fail(UD_EINVAL, "ud_score_batch_noalloc: " + std::to_string(n) + " poses exceed the limit of " +
+                                      std::to_string(UD_NOALLOC_MAX_POSES) + "; split the batch");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        if (c->ligs_dirty)
+            throw Fail(UD_ESTATE, "ud_score_batch_noalloc: the ligand set changed since it was last uploaded; "
+                                  "make one ud_score_batch, ud_search or ud_dock call first");
+        Env env = make_env(c, mode);
+        long long xs = 0, gs = 0;
+        int wsm = 0;
+        for (int i = 0; i < n; i++) {
+            const int l = pose_lig[i];
+            if (l < 0 || l >= (int)c->h_ligs.size()) throw Fail(UD_EINVAL, "pose ligand index out of range");
+            xs += 3LL * c->h_ligs[l].natom;
+            gs += 6 + c->h_ligs[l].ntors;
+            wsm = std::max(wsm, lig_ws(c->h_ligs[l]));
+        }
+        const size_t o_lig = 0;
+        const size_t o_xo = align256(o_lig + (size_t)n * sizeof(int));
+        const size_t o_go = align256(o_xo + (size_t)n * sizeof(long long));
+        const size_t o_x = align256(o_go + (size_t)n * sizeof(long long));
+        const size_t o_c = align256(o_x + (size_t)xs * sizeof(float));
+        const size_t o_r = align256(o_c + 3 * (size_t)n * sizeof(float));
+        const size_t o_e = align256(o_r + 3 * (size_t)n * sizeof(float));
+        const size_t o_g = align256(o_e + (size_t)n * sizeof(float));
+        const size_t end = o_g + (size_t)gs * sizeof(float);
+        if (end > (size_t)UD_NOALLOC_SCRATCH_BYTES)
+            throw Fail(UD_EINVAL, "ud_score_batch_noalloc: the batch needs " + std::to_string(end) +
+                                      " bytes of staging, above the fixed " +
+                                      std::to_string((size_t)UD_NOALLOC_SCRATCH_BYTES) + "; split the batch");
+        unsigned char* s = noalloc_scratch(c->device);
+        int* d_lig = reinterpret_cast<int*>(s + o_lig);
+        long long* d_xo = reinterpret_cast<long long*>(s + o_xo);
+        long long* d_go = reinterpret_cast<long long*>(s + o_go);
+        float* d_x = reinterpret_cast<float*>(s + o_x);
+        float* d_c = reinterpret_cast<float*>(s + o_c);
+        float* d_r = reinterpret_cast<float*>(s + o_r);
+        float* d_e = reinterpret_cast<float*>(s + o_e);
+        float* d_g = reinterpret_cast<float*>(s + o_g);
+        cudaStream_t st = c->stream;
+        ck(cudaMemcpyAsync(d_lig, pose_lig, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
+        ck(cudaMemcpyAsync(d_x, coords, (size_t)xs * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
+        ck(cudaMemcpyAsync(d_c, centers, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
+        ck(cudaMemcpyAsync(d_r, rotvecs, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st), "H2D");
+        // every offset, energy and gradient word is written below: nothing has to start at zero
+        k_pose_offsets<<<1, 1024, 0, st>>>(c->d_ligs.p, n, d_lig, d_xo, d_go);
+        ck(cudaGetLastError(), "k_pose_offsets launch");
+        const int W = pick_warps(c, wsm, 0, 8);
+        const size_t smem = (size_t)W * wsm * 4;
+        set_smem(k_score, smem);
+        PoseIO io{d_lig, d_xo, d_x, d_c, d_r, d_go};
+        k_score<<<(n + W - 1) / W, 32 * W, smem, st>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, d_e,
+                                                       d_g);
+        ck(cudaGetLastError(), "k_score launch");
+        ck(cudaMemcpyAsync(out_e, d_e, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaMemcpyAsync(out_g, d_g, (size_t)gs * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
+        ck(cudaStreamSynchronize(st), "k_score");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}

@@ -62,6 +62,7 @@ def load_library() -> C.CDLL:
         "ud_ligand_count": ([vp], i),
         "ud_record_floats": ([vp, i], i),
         "ud_score_batch": ([vp, i, ip, fp, fp, fp, i, f, f, fp, fp], i),
+        "ud_score_batch_noalloc": ([vp, i, ip, fp, fp, fp, i, f, f, fp, fp], i),
         "ud_score_terms": ([vp, i, ip, fp, i, fp, fp], i),
         "ud_bfgs_batch": ([vp, i, ip, fp, i, i, f, f, i, i, ip], i),
         "ud_search": ([vp, C.c_uint64, i, i, i, i, i, C.POINTER(C.c_longlong)], i),
@@ -254,6 +255,22 @@ class Engine:
         g = np.zeros(int(sum(dims)), np.float32)
         self._check(self.L.ud_score_batch(self.h, len(pl), _p(pl), _p(x), _p(ce), _p(rv), int(mode), float(vcap),
                                           float(slope), _p(e), _p(g)))
+        gs = np.split(g, np.cumsum(dims)[:-1]) if len(dims) > 1 else [g]
+        return e, gs
+
+    def score_batch_noalloc(self, pose_lig: Sequence[int], coords: Sequence[np.ndarray], centers, rotvecs,
+                            mode: int = MODE_GRID, vcap: float = 1e30, slope: float = 1e6):
+        """score_batch through ud_score_batch_noalloc: no device allocation inside the call;
+        staging in the library's fixed per-device array (limits in include/udock_b200.h)."""
+        pl = np.ascontiguousarray(pose_lig, np.int32)
+        x = np.ascontiguousarray(np.concatenate([np.asarray(c, np.float32).reshape(-1) for c in coords]))
+        ce = np.ascontiguousarray(centers, np.float32).reshape(-1)
+        rv = np.ascontiguousarray(rotvecs, np.float32).reshape(-1)
+        dims = [6 + self.ligands[l].ntors for l in pl]
+        e = np.zeros(len(pl), np.float32)
+        g = np.zeros(int(sum(dims)), np.float32)
+        self._check(self.L.ud_score_batch_noalloc(self.h, len(pl), _p(pl), _p(x), _p(ce), _p(rv), int(mode),
+                                                  float(vcap), float(slope), _p(e), _p(g)))
         gs = np.split(g, np.cumsum(dims)[:-1]) if len(dims) > 1 else [g]
         return e, gs
 
