@@ -58,12 +58,28 @@ enum BlobHdr {
     H_GOFF,        // natom+1 ints: per-atom lists of (pair index, partner) for the gather
     H_GADJ,        // entries: pair index | partner << 16
     H_TOTAL,
+    H_STAGE,       // words of the blob prefix the search stages into shared memory
     H_WORDS = 36
 };
 constexpr int AF_HEAVY = 1, AF_HYD = 2, AF_ACC = 4, AF_DON = 8;
+// inlining of the large routines of the search loop: a single shared copy (noinline)
+// keeps the loop's instruction footprint small, inlining saves the call overhead
+#ifndef UD_EVAL_ATTR
+#define UD_EVAL_ATTR __forceinline__
+#endif
+#ifndef UD_KIN_ATTR
+#define UD_KIN_ATTR __forceinline__
+#endif
+#ifndef UD_LS_ATTR
+#define UD_LS_ATTR __forceinline__
+#endif
 #ifndef RR32_MAX_ATOMS
 #define RR32_MAX_ATOMS 32      // ligands up to this size use the register round robin (<= 32)
 #endif
+// intra-pair path of a ligand of n atoms: 0 register round robin (one atom per lane),
+// 2 the pair list (pair buffer or atomics).  A round robin with two atoms per lane was
+// measured 1.5x slower on the search than the pair buffer (shuffle-bound, spills).
+__host__ __device__ __forceinline__ int intra_path(int n) { return n <= RR32_MAX_ATOMS ? 0 : 2; }
 constexpr int PREC_HYD = 1 << 24, PREC_HB = 1 << 25;
 constexpr int PAIR_ZERO = 1 << 16, PAIR_HYD = 1 << 17, PAIR_HB = 1 << 18;
 
@@ -326,7 +342,9 @@ __device__ __forceinline__ void rotvec_to_quat(float vx, float vy, float vz, flo
     float th = sqrtf(vx * vx + vy * vy + vz * vz);
     if (th > EPS_F) {
         float s, c;
-        sincosf(th * 0.5f, &s, &c);
+        const float h = th * 0.5f;
+        if (h <= PI_F) __sincosf(h, &s, &c);     // hardware sine/cosine on [0, pi]
+        else sincosf(h, &s, &c);
         const float k = __fdividef(s, th);
         q0 = c;
         q1 = k * vx;
@@ -368,12 +386,12 @@ __device__ __forceinline__ RotGradBasis rot_grad_basis(float vx, float vy, float
     if (ang > EPS_F) {
         th = normalize_angle_2pi(ang);
         if (th > PI_F) { th = 2.f * PI_F - th; ang = -ang; }
-        B.vb0 = vx / ang; B.vb1 = vy / ang; B.vb2 = vz / ang;
+        B.vb0 = __fdividef(vx, ang); B.vb1 = __fdividef(vy, ang); B.vb2 = __fdividef(vz, ang);
     } else {
         th = 0.f; B.vb0 = B.vb1 = B.vb2 = 0.f;
     }
-    sincosf(th, &B.s, &B.c);
-    if (th > EPS_F) { B.sdt = B.s / th; B.omc = (1.f - B.c) / th; }
+    __sincosf(th, &B.s, &B.c);                   // th in [0, pi]
+    if (th > EPS_F) { B.sdt = __fdividef(B.s, th); B.omc = __fdividef(1.f - B.c, th); }
     else { float t2 = th * th; B.sdt = 1.f - t2 / 6.f; B.omc = th / 2.f - th * t2 / 24.f; }
     return B;
 }
@@ -476,13 +494,15 @@ __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x
 // intra energy.  The kernel is issue bound, so each variant keeps the number of
 // evaluated pair slots close to the number of pairs.
 
-// natom <= 32: a round robin in registers.  Lane a owns atom a; in round t = 1..16 it
-// pairs with atom (a + t) mod 32, fetched by shuffle (at t = 16 only a < 16 computes),
-// keeps the force on its own atom and hands the reaction back by shuffle.  Every pair is
-// visited once; no shared memory, no atomics, fixed summation order.
+// natom = n <= 32: a round robin in registers.  Lane a < n owns atom a; in round
+// t = 1..n/2 it pairs with atom (a + t) mod n, fetched by shuffle (in the last round of an
+// even n only a < n/2 computes), keeps the force on its own atom and hands the reaction
+// back by shuffle.  Every pair is visited once in n/2 rounds; no shared memory, no
+// atomics, fixed summation order.
 __device__ __forceinline__ float intra_rr32(const Topo& T, const float* X, float* F, float vcap) {
     const int a = lane_id();
-    const bool va = a < T.natom;
+    const int n = T.natom;
+    const bool va = a < n;
     float xa = 0.f, ya = 0.f, za = 0.f, Ra = 0.f;
     int fa = 0;
     unsigned ma = 0u;
@@ -490,19 +510,23 @@ __device__ __forceinline__ float intra_rr32(const Topo& T, const float* X, float
         xa = X[3 * a]; ya = X[3 * a + 1]; za = X[3 * a + 2];
         Ra = T.radius(a); fa = T.aflags(a); ma = T.pmask(a);
     }
+    const int rounds = n >> 1;
+    const int half = (n & 1) ? WARP : rounds;          // last round of an even n: a < n/2 only
     float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
 #pragma unroll 1
-    for (int t = 1; t <= 16; t++) {
-        const int b = (a + t) & 31;
+    for (int t = 1; t <= rounds; t++) {
+        int b = a + t, src = a - t;                    // partner, and the lane that paired with a
+        if (b >= n) b -= n;
+        if (src < 0) src += n;
+        if (!va) { b = a; src = a; }
         const float xb = __shfl_sync(FULL, xa, b), yb = __shfl_sync(FULL, ya, b), zb = __shfl_sync(FULL, za, b);
         const float Rb = __shfl_sync(FULL, Ra, b);
         const int fb = __shfl_sync(FULL, fa, b);
         const float dx = xb - xa, dy = yb - ya, dz = zb - za;
         float sc = 0.f;
-        if (((ma >> b) & 1u) && (t < 16 || a < 16))
+        if (((ma >> b) & 1u) && (t < rounds || a < half))
             e += pair_scalar(dx, dy, dz, Ra + Rb, flags_hyd(fa, fb), flags_hb(fa, fb), vcap, sc);
         const float px = -sc * dx, py = -sc * dy, pz = -sc * dz;       // force on a
-        const int src = (a - t) & 31;                                  // the lane that paired with a
         fx += px - __shfl_sync(FULL, px, src);
         fy += py - __shfl_sync(FULL, py, src);
         fz += pz - __shfl_sync(FULL, pz, src);
@@ -613,7 +637,8 @@ __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const f
         F[3 * i] = fx; F[3 * i + 1] = fy; F[3 * i + 2] = fz;
     }
     __syncwarp();
-    if (T.natom <= RR32_MAX_ATOMS) energy += intra_rr32(T, X, F, vcap);
+    const int path = intra_path(T.natom);
+    if (path == 0) energy += intra_rr32(T, X, F, vcap);
     else if (PB) energy += intra_buffered(T, X, F, vcap, PB);
     else energy += intra_atomic(T, X, F, vcap);
     // bias (bfgs.cuh:356-388; vina.h:353-400)
@@ -707,7 +732,7 @@ __device__ __forceinline__ void grad_from_forces(const Topo& T, const Env& env, 
     __syncwarp();
 }
 
-__device__ __forceinline__ float eval_e_grad(const Topo& T, const Env& env, Slot P, float* F, float* G,
+__device__ UD_EVAL_ATTR float eval_e_grad(const Topo& T, const Env& env, Slot P, float* F, float* G,
                                              float vcap, float slope, float* PB) {
     float e = eval_e_f(T, env, P.x, F, vcap, slope, PB);
     grad_from_forces(T, env, P, F, G);
@@ -722,7 +747,8 @@ __device__ __forceinline__ void refresh_center(const Topo& T, Slot P) {
     s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2);
     __syncwarp();
     if (lane == 0) {
-        P.h[1] = s0 / T.natom; P.h[2] = s1 / T.natom; P.h[3] = s2 / T.natom;
+        const float n = (float)T.natom;
+        P.h[1] = __fdividef(s0, n); P.h[2] = __fdividef(s1, n); P.h[3] = __fdividef(s2, n);
     }
     __syncwarp();
 }
@@ -746,9 +772,9 @@ __device__ __forceinline__ void rotate_torsion(const Topo& T, Slot P, int k, flo
     const int from = T.axis(2 * k), to = T.axis(2 * k + 1);
     const float tx = P.x[3 * to], ty = P.x[3 * to + 1], tz = P.x[3 * to + 2];
     float ax = tx - P.x[3 * from], ay = ty - P.x[3 * from + 1], az = tz - P.x[3 * from + 2];
-    const float l = sqrtf(ax * ax + ay * ay + az * az);
-    if (l <= EPS_F) { ax = 1.f; ay = 0.f; az = 0.f; }
-    else { ax /= l; ay /= l; az /= l; }
+    const float l2 = ax * ax + ay * ay + az * az;
+    if (!(l2 > EPS_F * EPS_F)) { ax = 1.f; ay = 0.f; az = 0.f; }
+    else { const float il = rsqrtf(l2); ax *= il; ay *= il; az *= il; }
     __syncwarp();
     const int q1 = T.rot_off(k + 1);
     for (int q = T.rot_off(k) + lane; q < q1; q += WARP) {
@@ -779,7 +805,7 @@ __device__ __forceinline__ void apply_dihe(const Topo& T, Slot P, int k, float i
 // translation (bfgs.cuh:560-618).  SC holds 2 floats per torsion of scratch.  The
 // dihedral updates are independent of the coordinates, so they run lane-parallel first;
 // the rotations then follow sequentially in index order as in the reference.
-__device__ __forceinline__ void apply_update(const Topo& T, const Env& env, Slot P, const float* G, float alpha,
+__device__ UD_KIN_ATTR void apply_update(const Topo& T, const Env& env, Slot P, const float* G, float alpha,
                                              float* SC) {
     const int lane = lane_id();
     for (int k = lane; k < T.ntors; k += WARP) {
@@ -843,7 +869,7 @@ __device__ __forceinline__ void minus_hv(const double* H, const float* v, float*
 }
 
 // Backtracking Armijo line search (bfgs.cuh:623-670).  Trial poses go to Pn.
-__device__ __forceinline__ float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, const Work& W,
+__device__ UD_LS_ATTR float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, const Work& W,
                                              int dim, float e0, float vcap, float slope, float& alpha_out,
                                              int& n_eval) {
     float alpha = 1.f, e_new = 0.f;
@@ -904,14 +930,13 @@ __device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots,
         const double r = 1.0 / ((double)alpha * (double)yp);
         const double a = alpha;
         const double c1 = a * r, c2 = a * a * (r * r * yhy + r);
+        int i = lane, j = 0;                                  // idx = i + j(j+1)/2, i <= j
+        while (i > j) { j++; i -= j; }
         for (int idx = lane; idx < ntri; idx += WARP) {
-            // idx = i + j(j+1)/2, i <= j
-            int j = (int)((sqrtf(8.f * (float)idx + 1.f) - 1.f) * 0.5f);
-            j -= (j * (j + 1) / 2 > idx);
-            j += ((j + 1) * (j + 2) / 2 <= idx);
-            const int i = idx - j * (j + 1) / 2;
             const double pi = W.p[i], pj = W.p[j];
             W.H[idx] += c1 * ((double)W.mhy[i] * pj + (double)W.mhy[j] * pi) + c2 * pi * pj;
+            i += WARP;
+            while (i > j) { j++; i -= j; }
         }
         __syncwarp();
     }

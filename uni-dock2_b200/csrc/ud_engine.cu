@@ -32,16 +32,13 @@ static const float kVdwHost[NT] = {1.1f, 1.92f, 1.9f, 1.9f, 1.8f, 1.8f, 1.8f, 1.
 // ====================================================================== layout helpers
 __host__ __device__ inline int r4(int x) { return (x + 3) & ~3; }
 __host__ __device__ inline int rec_floats(int n, int t) { return r4(8 + 3 * n + t); }
-// pair buffer floats of a ligand: used above 32 atoms while the pair list fits PB_MAX
+// pair buffer floats of a ligand: used on the pair-list path while the list fits PB_MAX
 #ifndef PB_MAX_FLOATS
 #define PB_MAX_FLOATS 4096
 #endif
-#ifndef PB_MIN_ATOMS
-#define PB_MIN_ATOMS RR32_MAX_ATOMS
-#endif
 constexpr int PB_MAX = PB_MAX_FLOATS;
 __host__ __device__ inline int pb_floats(int n, int npair) {
-    return (n > PB_MIN_ATOMS && npair <= PB_MAX) ? r4(npair) : 0;
+    return (intra_path(n) == 2 && npair <= PB_MAX) ? r4(npair) : 0;
 }
 __host__ __device__ inline int ws_floats(int n, int t, int npair) {
     int d = 6 + t;
@@ -54,7 +51,7 @@ struct LigDev {
     int natom, ntors, nheavy;
     int stride;          // record floats
     int lig_uid;
-    int pad;
+    int stage_words;     // blob prefix the search stages into shared memory
     long long best_off;  // float offset of chain 0's record in the chain-pose buffer
     long long out_off;   // float offset of the output records (num_pose capacity)
 };
@@ -365,9 +362,6 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
 }
 
 // ====================================================================== MC search
-#ifndef SEARCH_MIN_BLOCKS
-#define SEARCH_MIN_BLOCKS 4          // 256-thread CTAs per SM the register budget is sized for
-#endif
 struct SearchP {
     uint32_t k0, k1;
     int nchain, mc_steps, opt_steps, randomize;
@@ -382,11 +376,14 @@ __device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp,
 
 __device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
 
-// Work items are (ligand, first chain, chain count <= warps per CTA) in descending ligand
-// cost; CTAs take items from a global counter, re-stage the topology blob only when the
-// ligand changes, and their warps take the item's chains from a shared counter.  Large
-// ligands are so spread over many CTAs and the launch ends with the cheapest items.
-__global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __restrict__ blobs,
+// Work items are (ligand, first chain, chain count) in descending ligand cost; CTAs take
+// items from a global counter, re-stage the topology blob only when the ligand changes,
+// and their warps take the item's chains from a shared counter.  Large ligands are so
+// spread over many CTAs and the launch ends with the cheapest items.
+// MINB: 256-thread CTAs per SM the register budget is sized for (4: 64 registers, 3: 80);
+// the host picks the instantiation whose CTA count the shared memory allows.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ blobs,
                                                 const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                 int nitems, Env env, SearchP sp, float* best, int* work_counter,
                                                 unsigned long long* nevals) {
@@ -406,7 +403,7 @@ __global__ void __launch_bounds__(256, SEARCH_MIN_BLOCKS) k_search(const int* __
         const int4 item = items[it];          // (ligand, first chain, count, -)
         const LigDev L = ligs[item.x];
         if (item.x != s_lig) {
-            for (int w = threadIdx.x; w < L.blob_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+            for (int w = threadIdx.x; w < L.stage_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
         }
         __syncthreads();
         if (threadIdx.x == 0) s_lig = item.x;
@@ -646,7 +643,7 @@ struct DBuf {
 };
 
 struct LigHost {
-    int natom, ntors, nheavy, blob_words, stride, nprec;
+    int natom, ntors, nheavy, blob_words, stride, nprec, stage_words;
     long long blob_off;
 };
 inline int lig_ws(const LigHost& h) { return ws_floats(h.natom, h.ntors, h.nprec); }
@@ -675,7 +672,7 @@ struct ud_ctx {
     DBuf<int> d_blobs;
     DBuf<LigDev> d_ligs;
     bool ligs_dirty = true;
-    int max_natom = 0, max_ntors = 0, max_blob = 0;
+    int max_natom = 0, max_ntors = 0, max_blob = 0, max_stage = 0;
     // search state
     int nchain = 0;
     long long best_floats = 0;
@@ -743,7 +740,7 @@ void sync_ligs(ud_ctx* c) {
         d.nheavy = h.nheavy;
         d.stride = h.stride;
         d.lig_uid = (int)i;
-        d.pad = 0;
+        d.stage_words = h.stage_words;
         d.best_off = 0;
         d.out_off = 0;
     }
@@ -969,23 +966,6 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 if (v < 0 || v >= n) throw Fail(UD_EINVAL, "rotated atom out of range");
                 blob[o + k] = v;
             }
-            o = put(H_PAIR_OFF, n + 1);
-            for (int i = 0; i <= n; i++) blob[o + i] = pair_off[a0 + i] - p0;
-            o = put(H_PAIRS, np);
-            for (int i = 0; i < n; i++) {
-                const int ti = types[a0 + i];
-                for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++) {
-                    int v = pairs[p0 + k];
-                    if (v < 0 || v >= n) throw Fail(UD_EINVAL, "intra pair atom out of range");
-                    const int tj = types[a0 + v];
-                    const unsigned b1 = 1u << ti, b2 = 1u << tj;
-                    int ent = v;
-                    if (ti == VN_H || tj == VN_H) ent |= PAIR_ZERO;
-                    if ((b1 & HYD_MASK) && (b2 & HYD_MASK)) ent |= PAIR_HYD;
-                    if (((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK))) ent |= PAIR_HB;
-                    blob[o + k] = ent;
-                }
-            }
             o = put(H_BIAS_OFF, n + 1);
             for (int i = 0; i <= n; i++) blob[o + i] = bias_off ? bias_off[a0 + i] - b0 : 0;
             o = put(H_BIAS, 5 * nb);
@@ -1030,8 +1010,11 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 // each atom about twice
                 std::vector<char> scored((size_t)n * n, 0);
                 for (int i = 0; i < n; i++)
-                    for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++)
-                        scored[(size_t)i * n + pairs[p0 + k]] = 1;
+                    for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++) {
+                        const int v = pairs[p0 + k];
+                        if (v < 0 || v >= n) throw Fail(UD_EINVAL, "intra pair atom out of range");
+                        scored[(size_t)i * n + v] = 1;
+                    }
                 std::vector<int> rec;
                 for (int t = 1; t <= n / 2; t++)
                     for (int a = 0; a < n; a++) {
@@ -1053,8 +1036,9 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 const int np2 = (int)rec.size() / 2;
                 if (np2 > 0xFFFF) throw Fail(UD_EINVAL, "too many intra pairs (max 65535)");
                 blob[H_NPREC] = np2;
-                o = put(H_PREC, (int)rec.size());
-                for (size_t q = 0; q < rec.size(); q++) blob[o + q] = rec[q];
+                // sections the search reads come first: what the register round robin needs
+                // (ligands of at most 32 atoms), then the pair list and gather lists of larger
+                // ligands, then the adjacency only the final scoring reads (not staged)
                 o = put(H_AFLAGS, n);
                 for (int i = 0; i < n; i++) {
                     const int t = types[a0 + i];
@@ -1062,14 +1046,17 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                     blob[o + i] = (t != VN_H ? AF_HEAVY : 0) | ((b & HYD_MASK) ? AF_HYD : 0) |
                                   ((b & ACC_MASK) ? AF_ACC : 0) | ((b & DON_MASK) ? AF_DON : 0);
                 }
-                // partner masks for the register round robin (ligands of at most 32 atoms)
-                o = put(H_PMASK, n <= 32 ? n : 0);
-                if (n <= 32)
+                const bool rr = intra_path(n) == 0;      // partner masks for the round robin
+                o = put(H_PMASK, rr ? n : 0);
+                if (rr)
                     for (int p = 0; p < np2; p++) {
                         const int i = rec[2 * p] & 0xFFF, j = (rec[2 * p] >> 12) & 0xFFF;
                         blob[o + i] |= (int)(1u << j);
                         blob[o + j] |= (int)(1u << i);
                     }
+                const int stage_small = (int)blob.size();
+                o = put(H_PREC, (int)rec.size());
+                for (size_t q = 0; q < rec.size(); q++) blob[o + q] = rec[q];
                 // gather lists: for each atom, (pair index, partner) in pair-index order
                 std::vector<std::vector<int>> g(n);
                 for (int p = 0; p < np2; p++) {
@@ -1084,11 +1071,29 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 o = put(H_GADJ, acc);
                 for (int i = 0, k = 0; i < n; i++)
                     for (int v : g[i]) blob[o + k++] = v;
+                blob[H_STAGE] = rr ? stage_small : (int)blob.size();
+            }
+            o = put(H_PAIR_OFF, n + 1);
+            for (int i = 0; i <= n; i++) blob[o + i] = pair_off[a0 + i] - p0;
+            o = put(H_PAIRS, np);
+            for (int i = 0; i < n; i++) {
+                const int ti = types[a0 + i];
+                for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++) {
+                    const int v = pairs[p0 + k];
+                    const int tj = types[a0 + v];
+                    const unsigned b1 = 1u << ti, b2 = 1u << tj;
+                    int ent = v;
+                    if (ti == VN_H || tj == VN_H) ent |= PAIR_ZERO;
+                    if ((b1 & HYD_MASK) && (b2 & HYD_MASK)) ent |= PAIR_HYD;
+                    if (((b1 & ACC_MASK) && (b2 & DON_MASK)) || ((b1 & DON_MASK) && (b2 & ACC_MASK))) ent |= PAIR_HB;
+                    blob[o + k] = ent;
+                }
             }
             blob[H_TOTAL] = (int)blob.size();
             LigHost h;
             h.natom = n; h.ntors = T; h.nheavy = nheavy;
             h.blob_words = (int)blob.size();
+            h.stage_words = blob[H_STAGE];
             h.blob_off = (long long)c->h_blobs.size();
             h.stride = rec_floats(n, T);
             h.nprec = blob[H_NPREC];
@@ -1097,6 +1102,7 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
             c->max_natom = std::max(c->max_natom, n);
             c->max_ntors = std::max(c->max_ntors, T);
             c->max_blob = std::max(c->max_blob, h.blob_words);
+            c->max_stage = std::max(c->max_stage, h.stage_words);
         }
         c->ligs_dirty = true;
         c->has_results = false;
@@ -1111,7 +1117,7 @@ int ud_clear_ligands(ud_ctx* c) {
     c->h_blobs.clear();
     c->h_ligs.clear();
     c->h_ligdev.clear();
-    c->max_natom = c->max_ntors = c->max_blob = 0;
+    c->max_natom = c->max_ntors = c->max_blob = c->max_stage = 0;
     c->ligs_dirty = true;
     c->has_results = false;
     c->nchain = 0;
@@ -1289,15 +1295,29 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
         cost[l] = (np + 8.0 * h.natom + 40.0 * h.ntors + 200.0) * (6 + h.ntors);
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    int blob_max = r4(c->max_blob);
+    int blob_max = r4(c->max_stage);
     int W = pick_warps(c, wsm, blob_max, 8);
     size_t smem = ((size_t)blob_max + (size_t)W * wsm) * 4;
-    // one chain per warp per item: a CTA finishes an item in one chain time, so small
-    // batches still fill every resident CTA and the tail is one chain long
+    int smem_sm = 0;
+    ck(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device), "attribute");
+    // CTAs per SM the shared memory allows (1 KB per CTA is reserved by the runtime)
+    const bool four = (size_t)smem_sm / (smem + 1024) >= 4;
+    auto kern = four ? k_search<4> : k_search<3>;
+    set_smem(kern, smem);
+    int per_sm = 0;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem), "occupancy");
+    if (per_sm < 1) per_sm = 1;
+    const long long resident = (long long)c->nsm * per_sm;
+    // k chains per warp per item (W*k chains): the warps of a CTA share an item's chains
+    // dynamically, so the wait at the item's end for its slowest chain shrinks with k;
+    // k stays small enough that every resident CTA gets at least two items
+    const long long total_chains = (long long)nlig * nchain;
+    const int k = (int)std::max(1LL, std::min(4LL, total_chains / std::max(1LL, 2 * resident * W)));
+    const int item_chains = W * k;
     std::vector<int4> items;
     for (int l : order)
-        for (int c0 = 0; c0 < nchain; c0 += W)
-            items.push_back(make_int4(l, c0, std::min(W, nchain - c0), 0));
+        for (int c0 = 0; c0 < nchain; c0 += item_chains)
+            items.push_back(make_int4(l, c0, std::min(item_chains, nchain - c0), 0));
     upload_ligdev(c);
     c->best_floats = tot;
     c->d_best.ensure((size_t)tot);
@@ -1308,11 +1328,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
     ck(cudaMemsetAsync(c->d_nevals.p, 0, 2 * sizeof(unsigned long long), c->stream), "memset");
     c->counters[3] = (long long)nlig * nchain;
-    set_smem(k_search, smem);
-    int per_sm = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, 32 * W, smem), "occupancy");
-    if (per_sm < 1) per_sm = 1;
-    int grid = std::min(nitems, c->nsm * per_sm);
+    int grid = (int)std::min((long long)nitems, resident);
     SearchP sp;
     sp.k0 = (uint32_t)seed;
     sp.k1 = (uint32_t)(seed >> 32) ^ 0x5DEECE66u;
@@ -1323,7 +1339,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     sp.ws_max = wsm;
     sp.blob_max = blob_max;
     if (grid > 0) {
-        k_search<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, nitems, env, sp,
+        kern<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, nitems, env, sp,
                                                     c->d_best.p, c->d_counter.p, c->d_nevals.p);
         ck(cudaGetLastError(), "k_search launch");
         c->counters[2]++;
