@@ -216,6 +216,50 @@ int ud_stage_times(const ud_ctx* ctx, float* out6);
  * (src/cuda/common.cu:6, src/cuda/mc.cu:443). */
 int ud_counters(const ud_ctx* ctx, long long* out4);
 
+/* ---------------------------------------------------------------------------------------
+ * Learned move proposal.  No reference counterpart: a BF16 MLP (672 -> 256 -> 256 -> 256
+ * -> 64, ReLU, FP32 accumulation on the tensor cores) predicts from a chain's accepted
+ * pose a Gaussian (mean, log-variance) over its 6 + T move dimensions [centre shift (3),
+ * rotation vector (3), torsion changes (T)]; a sampled move replaces the random draw of
+ * mutate_pose_tile (src/cuda/mc.cu:146-256) with probability p_learned.  BFGS, Vina
+ * scoring and Metropolis stay as in the plain search.
+ * Features of a pose (672): energies of the first 8 grid maps at each of up to 80 atoms,
+ * squashed v/(1+|v|); torsion angles / pi (up to 20); E/(10+|E|); 1; zero padding.
+ * Parameters (flat FP32, ud_mlp_param_count of them): W1[672x256], b1, W2[256x256], b2,
+ * W3[256x256], b3, W4[256x64], b4; W row-major [in x out].  Output row (64): mean[0:26],
+ * raw log-variance[26:52] (clamped to [-8, 4] where used), 12 unused. */
+long long ud_mlp_param_count(void);
+/* He-normal weights (last layer scaled by 0.1), zero biases, Adam state cleared. */
+int ud_mlp_init(ud_ctx* ctx, uint64_t seed);
+int ud_mlp_set_params(ud_ctx* ctx, const float* params);
+int ud_mlp_get_params(ud_ctx* ctx, float* params);
+/* out[n x 64] for features x[n x 672]. */
+int ud_mlp_forward(ud_ctx* ctx, int n, const float* x, float* out);
+/* Mean masked Gaussian negative log-likelihood of targets y[n x 26] under mask[n x 26],
+ * and its gradient with respect to every parameter (flat, param_count floats). */
+int ud_mlp_loss_grad(ud_ctx* ctx, int n, const float* x, const float* y, const float* mask, double* out_loss,
+                     float* out_grad);
+/* Adam (lr; betas 0.9, 0.999; eps 1e-8) over shuffled full minibatches for `epochs`;
+ * out_epoch_loss[epochs] (nullable) receives the mean minibatch loss of each epoch. */
+int ud_mlp_train(ud_ctx* ctx, int n, const float* x, const float* y, const float* mask, int epochs, int batch,
+                 float lr, uint64_t seed, float* out_epoch_loss);
+/* The MC search of ud_search with learned moves (grid scoring; ligands of at most 80
+ * atoms and 20 torsions): every MC step is one launch of all chains, after one batched
+ * forward pass of the network over every chain's accepted pose.  p_learned = 0 gives
+ * exactly ud_search's chains.  Results as ud_search (ud_get_chain_poses, ud_cluster). */
+int ud_search_learned(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
+                      float p_learned, long long* out_nevals);
+/* Run the plain search (as ud_search_learned with p_learned = 0) and record up to
+ * max_moves accepted moves: the features of the pose before the step, the move to the
+ * accepted pose (centre shift, rotation vector of a rigid frame of the ligand, wrapped
+ * torsion changes) and the mask of the dimensions that apply.  Replaces nothing. */
+int ud_collect_moves(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
+                     int max_moves, int* out_count);
+/* Copy the first n recorded moves: x[n x 672], y[n x 26], mask[n x 26] (each nullable). */
+int ud_get_moves(ud_ctx* ctx, int n, float* out_x, float* out_y, float* out_mask);
+/* ud_mlp_train on the recorded moves, on the device. */
+int ud_mlp_train_moves(ud_ctx* ctx, int epochs, int batch, float lr, uint64_t seed, float* out_epoch_loss);
+
 #ifdef __cplusplus
 }
 #endif

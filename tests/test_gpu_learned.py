@@ -1,0 +1,132 @@
+"""GPU tests of the learned move proposal, through the C ABI.
+
+* forward pass, loss and every parameter gradient against the CPU oracle
+  (oracle/mlp_oracle.py restates the BF16 rounding points; remaining differences come from
+  FP32 summation order and from BF16 roundings of hidden values that sit on a rounding
+  boundary): outputs within 2e-2 absolute + 2e-2 relative, the loss within 1e-3
+  relative, each gradient block within 3e-2 of its norm;
+* training on the device lowers the loss;
+* the learned search with p_learned = 0 reproduces the fused search bit for bit;
+* recorded moves are consistent with the ligands (masks, wrapped torsion changes), and a
+  network trained on them runs in the search with finite, real energies.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from gpu_helpers import engine_for
+
+pytestmark = pytest.mark.gpu
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import mlp_oracle as M  # noqa: E402
+
+
+@pytest.fixture(scope="module")
+def bare_engine(small_system):
+    from ud2b200 import Engine
+    eng = Engine(small_system["box"])
+    yield eng
+    eng.close()
+
+
+def _data(rng, n):
+    X = rng.normal(0, 0.6, (n, M.IN)).astype(np.float32)
+    Y = rng.normal(0, 0.5, (n, M.NDIM)).astype(np.float32)
+    Mk = (rng.random((n, M.NDIM)) < 0.7).astype(np.float32)
+    return X, Y, Mk
+
+
+def test_param_count(bare_engine):
+    assert bare_engine.mlp_param_count() == M.param_count()
+
+
+def test_forward_matches_oracle(bare_engine):
+    rng = np.random.default_rng(1)
+    p = M.init_params(5)
+    p = (p + rng.normal(0, 0.01, p.size)).astype(np.float32)      # nonzero biases
+    bare_engine.mlp_set_params(p)
+    assert np.array_equal(bare_engine.mlp_get_params(), p)
+    X, _, _ = _data(rng, 97)                                          # not a tile multiple
+    got = bare_engine.mlp_forward(X)
+    want, _ = M.forward(p, X)
+    assert got.shape == (97, 64)
+    assert np.all(np.abs(got - want) <= 2e-2 + 2e-2 * np.abs(want)), float(np.max(np.abs(got - want)))
+
+
+def test_loss_and_gradient_match_oracle(bare_engine):
+    rng = np.random.default_rng(2)
+    p = M.init_params(6)
+    p = (p + rng.normal(0, 0.01, p.size)).astype(np.float32)
+    bare_engine.mlp_set_params(p)
+    X, Y, Mk = _data(rng, 130)
+    loss, g = bare_engine.mlp_loss_grad(X, Y, Mk)
+    want_loss, want_g = M.loss_grad(p, X, Y, Mk)
+    assert abs(loss - want_loss) <= 1e-3 * max(1.0, abs(want_loss)), (loss, want_loss)
+    off = 0
+    for shape in M.SHAPES:
+        n = int(np.prod(shape))
+        a, b = g[off:off + n].astype(np.float64), want_g[off:off + n]
+        err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert err <= 3e-2, (shape, err)
+        off += n
+
+
+def test_training_lowers_loss(bare_engine):
+    rng = np.random.default_rng(3)
+    X, _, Mk = _data(rng, 2048)
+    A = rng.normal(0, 0.05, (M.IN, M.NDIM))
+    Y = np.tanh(X @ A).astype(np.float32)                             # learnable targets
+    bare_engine.mlp_init(7)
+    l0, _ = bare_engine.mlp_loss_grad(X, Y, Mk)
+    losses = bare_engine.mlp_train(X, Y, Mk, epochs=8, batch=256, lr=1e-3, seed=1)
+    l1, _ = bare_engine.mlp_loss_grad(X, Y, Mk)
+    assert np.all(np.isfinite(losses))
+    assert l1 < l0 - 0.2, (l0, l1, losses)
+
+
+@pytest.fixture(scope="module")
+def search_sys(small_system):
+    eng, _ = engine_for(small_system)
+    yield dict(small_system, eng=eng)
+    eng.close()
+
+
+def test_learned_search_p0_matches_fused_search(search_sys):
+    eng = search_sys["eng"]
+    eng.search(seed=21, nchain=16, mc_steps=6, opt_steps=5, randomize=True)
+    want = [eng.chain_poses(l).copy() for l in range(len(search_sys["ligs"]))]
+    ne = eng.search_learned(seed=21, nchain=16, mc_steps=6, opt_steps=5, p_learned=0.0)
+    assert ne > 0
+    for l in range(len(search_sys["ligs"])):
+        got = eng.chain_poses(l)
+        assert np.array_equal(got, want[l]), l
+
+
+def test_collect_moves_and_learned_search(search_sys):
+    eng = search_sys["eng"]
+    ligs = search_sys["ligs"]
+    n = eng.collect_moves(seed=5, nchain=32, mc_steps=12, opt_steps=5, max_moves=4000)
+    assert 0 < n <= 4000
+    x, y, m = eng.get_moves(n)
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(y))
+    assert np.all(np.abs(x) <= 1.0 + 1e-6)                 # squashed features
+    assert np.all(x[:, 661] == 1.0)
+    assert np.all(np.abs(y[:, 6:]) <= np.pi + 1e-5)        # wrapped torsion changes
+    ntors = sorted(set(l.ntors for l in ligs))
+    dims = np.sum(m[:, 6:], axis=1).astype(int)
+    assert set(dims.tolist()) <= set(ntors)
+    assert np.all(m[:, :3] == 1.0)                          # free docking: centre shift applies
+    eng.mlp_init(3)
+    losses = eng.mlp_train_moves(epochs=6, batch=256, lr=1e-3, seed=2)
+    assert np.all(np.isfinite(losses)) and losses[-1] < losses[0]
+    ne = eng.search_learned(seed=9, nchain=16, mc_steps=8, opt_steps=5, p_learned=0.5)
+    assert ne > 0
+    from ud2b200 import split_record
+    for li, lig in enumerate(ligs):
+        recs = eng.chain_poses(li)
+        e = recs[:, 0]
+        assert np.all(np.isfinite(e)) and np.all(e < 1e8)
+        assert np.all(np.isfinite(recs))

@@ -59,6 +59,7 @@ enum BlobHdr {
     H_GADJ,        // entries: pair index | partner << 16
     H_TOTAL,
     H_STAGE,       // words of the blob prefix the search stages into shared memory
+    H_FRAME0,      // 3 words: non-collinear atoms no torsion moves (a rigid frame), or -1
     H_WORDS = 36
 };
 constexpr int AF_HEAVY = 1, AF_HYD = 2, AF_ACC = 4, AF_DON = 8;
@@ -297,7 +298,7 @@ __device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint
 __device__ __forceinline__ float u01(uint32_t u) {
     return (float)(u >> 8) * (1.0f / 16777216.0f) + (0.5f / 16777216.0f);
 }
-enum { P_WHICH = 0, P_TORS = 1, P_METRO = 2, P_SPHERE = 16, P_INIT = 256 };
+enum { P_WHICH = 0, P_TORS = 1, P_METRO = 2, P_LEARN = 3, P_LNORM = 8, P_SPHERE = 16, P_INIT = 256 };
 struct Rng {
     uint32_t k0, k1, chain, lig;
     __device__ __forceinline__ U4 draw(uint32_t step, uint32_t purpose) const {

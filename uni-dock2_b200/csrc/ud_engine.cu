@@ -20,7 +20,10 @@
 #include <algorithm>
 #include <stdexcept>
 #include <mutex>
+#include <random>
+#include <cuda_bf16.h>
 #include "ud_device.cuh"
+#include "ud_mlp.cuh"
 #include "../../include/udock_b200.h"
 
 using namespace ud;
@@ -376,6 +379,92 @@ __device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp,
 
 __device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
 
+// A learned move for one MC step: the proposal network's Gaussian (mean, raw log-variance
+// per dimension, 6 + T used) and the probability of taking it instead of a random move.
+struct Proposal {
+    const float* out;     // 64 floats: mean[0:26], raw log-variance[26:52]; null: random moves only
+    float p_learned;
+};
+
+// One MC step of a chain (mc.cu:323-393): the candidate (slot A+1) is the accepted pose
+// with one move applied (a random move, or a sample of the learned proposal), optimised by
+// BFGS with curl 10; Metropolis at T = 1.2 (step 0 always accepts); an accepted new best is
+// optimised again with curl 1000 and recorded.  Returns the accepted slot; sets *accepted.
+__device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws, int stride, int A, const Work& W,
+                                       const Rng& rng, int step, int opt_steps, int nrec, float* out, float& best_e,
+                                       int& ne, const Proposal& prop, bool& accepted) {
+    const int lane = lane_id();
+    const int C = (A + 1) & 3;
+    Slot SC = slot_at(ws, stride, C, T.natom);
+    slot_copy(SC, slot_at(ws, stride, A, T.natom), T.natom, T.ntors);
+    bool learned = false;
+    if (prop.out) learned = u01(rng.draw((uint32_t)step, P_LEARN).x) < prop.p_learned;
+    if (learned) {
+        // sample m ~ N(mean, exp(logvar)) per dimension (Box-Muller on Philox draws), clamp
+        // the rigid part to a sane step, apply as one update of the candidate
+        const int dim = 6 + T.ntors;
+        if (lane < dim) {
+            const U4 u = rng.draw((uint32_t)step, P_LNORM + (lane >> 2));
+            const uint32_t ua = (lane & 2) ? u.z : u.x, ub = (lane & 2) ? u.w : u.y;
+            const float r = sqrtf(-2.f * __logf(u01(ua))), th = 2.f * PI_F * u01(ub);
+            float sn, cs;
+            __sincosf(th, &sn, &cs);
+            const float z = (lane & 1) ? r * sn : r * cs;
+            const float lv = fminf(fmaxf(prop.out[26 + lane], -8.f), 4.f);
+            float m = prop.out[lane] + __expf(0.5f * lv) * z;
+            if (lane < 3) m = fminf(fmaxf(m, -4.f), 4.f);
+            else if (lane < 6) m = fminf(fmaxf(m, -PI_F), PI_F);
+            if (lane < 6 && env.constraint) m = 0.f;
+            if (!(m == m)) m = 0.f;
+            W.p[lane] = m;
+        }
+        __syncwarp();
+        apply_update(T, env, SC, W.p, 1.f, W.sc);
+    } else {
+        mutate(T, env, rng, (uint32_t)step, SC);
+    }
+    const float e_acc = ws[A * stride];
+    const float rx = u01(rng.draw((uint32_t)step, P_METRO).x);
+    accepted = false;
+    if (opt_steps == 0) {
+        float e = eval_e_grad(T, env, SC, W.F, W.g, VCAP_SEARCH, PENALTY_SLOPE, W.pb);
+        ne++;
+        if (lane == 0) SC.h[0] = e;
+        __syncwarp();
+        if (step == 0 || metropolis(e_acc, e, 1.2f, rx)) {
+            A = C;
+            accepted = true;
+            if (e < best_e) {
+                best_e = e;
+                store_record(out, SC, nrec);
+            }
+        }
+        return A;
+    }
+    // slots: A holds the accepted pose; the other three serve the candidate and the
+    // optimiser.  Both BFGS runs of a step (candidate with curl 10, accepted new best with
+    // curl 1000) go through one call site (phase 0 / 1).
+    for (int phase = 0; phase < 2; phase++) {
+        const int X = (A + 1 - phase) & 3;
+        const int R = bfgs(T, env, ws, stride, X, (X + 1) & 3, (X + 2) & 3, W, opt_steps,
+                           phase ? VCAP_AUTH : VCAP_SEARCH, PENALTY_SLOPE, ne);
+        const float e_new = ws[R * stride];
+        if (phase == 0) {
+            if (!(step == 0 || metropolis(e_acc, e_new, 1.2f, rx))) break;
+            A = R;
+            accepted = true;
+            if (!(e_new < best_e)) break;
+        } else {
+            A = R;
+            if (e_new < best_e) {
+                best_e = e_new;
+                store_record(out, slot_at(ws, stride, A, T.natom), nrec);
+            }
+        }
+    }
+    return A;
+}
+
 // Work items are (ligand, first chain, chain count) in descending ligand cost; CTAs take
 // items from a global counter, re-stage the topology blob only when the ligand changes,
 // and their warps take the item's chains from a shared counter.  Large ligands are so
@@ -431,49 +520,214 @@ __global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ bl
                 __syncwarp();
                 store_record(out, SA, nrec);
             } else {
-                // slots: A holds the accepted pose; the other three serve the candidate and
-                // the optimiser.  Both BFGS runs of a step (candidate with curl 10, accepted
-                // new best with curl 1000) go through one call site (phase 0 / 1).
-                for (int step = 0; step < sp.mc_steps; step++) {
-                    const int C = (A + 1) & 3;
-                    Slot SC = slot_at(ws, L.stride, C, T.natom);
-                    slot_copy(SC, slot_at(ws, L.stride, A, T.natom), T.natom, T.ntors);
-                    mutate(T, env, rng, (uint32_t)step, SC);
-                    const float e_acc = ws[A * L.stride];
-                    const float rx = u01(rng.draw((uint32_t)step, P_METRO).x);
-                    if (sp.opt_steps == 0) {
-                        float e = eval_e_grad(T, env, SC, W.F, W.g, VCAP_SEARCH, PENALTY_SLOPE, W.pb);
-                        ne++;
-                        if (lane == 0) SC.h[0] = e;
-                        __syncwarp();
-                        if (step == 0 || metropolis(e_acc, e, 1.2f, rx)) {
-                            A = C;
-                            if (e < best_e) {
-                                best_e = e;
-                                store_record(out, SC, nrec);
-                            }
-                        }
-                        continue;
-                    }
-                    for (int phase = 0; phase < 2; phase++) {
-                        const int X = (A + 1 - phase) & 3;
-                        const int R = bfgs(T, env, ws, L.stride, X, (X + 1) & 3, (X + 2) & 3, W, sp.opt_steps,
-                                           phase ? VCAP_AUTH : VCAP_SEARCH, PENALTY_SLOPE, ne);
-                        const float e_new = ws[R * L.stride];
-                        if (phase == 0) {
-                            if (!(step == 0 || metropolis(e_acc, e_new, 1.2f, rx))) break;
-                            A = R;
-                            if (!(e_new < best_e)) break;
-                        } else {
-                            A = R;
-                            if (e_new < best_e) {
-                                best_e = e_new;
-                                store_record(out, slot_at(ws, L.stride, A, T.natom), nrec);
-                            }
-                        }
-                    }
-                }
+                const Proposal none{nullptr, 0.f};
+                bool acc;
+                for (int step = 0; step < sp.mc_steps; step++)
+                    A = mc_step(T, env, ws, L.stride, A, W, rng, step, sp.opt_steps, nrec, out, best_e, ne, none, acc);
             }
+            my_evals += ne;
+            my_heavy += (unsigned long long)ne * T.nheavy;
+        }
+        __syncthreads();
+    }
+    if (lane == 0 && nevals) {
+        atomicAdd(nevals, my_evals);
+        atomicAdd(nevals + 1, my_heavy);
+    }
+}
+
+// ====================================================================== learned search
+// The same MC chains as k_search, advanced one step per launch so that every chain's move
+// can come from one batched evaluation of the proposal network: the accepted pose of each
+// chain stays in HBM (`acc`, laid out as the best records) between steps; a step is
+// k_learn_features -> network forward -> k_learn_step -> k_step_advance, captured once as
+// a CUDA graph and replayed mc_steps times.  With p_learned = 0 the chains follow exactly
+// the moves of k_search (same counter-based random stream, same step function).
+struct LearnP {
+    uint32_t k0, k1;
+    int nchain, opt_steps, randomize;
+    int ws_max, blob_max;
+    float p_learned;
+    int nfeat_maps;           // grid maps used as features (<= 8)
+};
+struct MoveSet {              // recorded accepted moves (training data)
+    __nv_bfloat16* x;         // [max][672] features of the pose before the move
+    float* y;                 // [max][26] move: centre shift, rotation vector, torsion changes
+    float* m;                 // [max][26] mask of the dimensions that apply
+    int* count;
+    int max;
+};
+
+// Features of a pose record (672 values): for each of up to 80 atoms the energies of the
+// first 8 grid maps at the atom, squashed v / (1 + |v|); torsion angles / pi; the pose's
+// energy squashed E / (10 + |E|); a constant 1.
+__device__ void pose_features(const Topo& T, const Env& env, const float* rec, int nmaps, __nv_bfloat16* row) {
+    const int lane = lane_id();
+    const float* x = rec + 8;
+    const float* d = rec + 8 + 3 * T.natom;
+    for (int i = lane; i < mlp::NATOM * mlp::NMAP; i += WARP) {
+        const int a = i >> 3, m = i & 7;
+        float v = 0.f;
+        if (a < T.natom && m < nmaps) {
+            float gx, gy, gz;
+            v = grid_sample(env.grid, m, x[3 * a], x[3 * a + 1], x[3 * a + 2], gx, gy, gz);
+            v = __fdividef(v, 1.f + fabsf(v));
+            if (!(v == v)) v = 0.f;
+        }
+        row[i] = __float2bfloat16_rn(v);
+    }
+    for (int k = lane; k < mlp::IN - mlp::NATOM * mlp::NMAP; k += WARP) {
+        float v = 0.f;
+        if (k < mlp::TMAX) v = k < T.ntors ? d[k] * (1.f / PI_F) : 0.f;
+        else if (k == mlp::TMAX) { const float e = rec[0]; v = __fdividef(e, 10.f + fabsf(e)); if (!(v == v)) v = 0.f; }
+        else if (k == mlp::TMAX + 1) v = 1.f;
+        row[mlp::NATOM * mlp::NMAP + k] = __float2bfloat16_rn(v);
+    }
+}
+
+__global__ void k_learn_features(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int nlig, int nchain,
+                                 Env env, const float* __restrict__ acc, const int* __restrict__ step_p, int nmaps,
+                                 __nv_bfloat16* __restrict__ X) {
+    if (*step_p == 0) return;                      // no accepted pose before the first step
+    const long long nch = (long long)nlig * nchain;
+    const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long g = w0; g < nch; g += nw) {
+        const int lig = (int)(g / nchain), c = (int)(g % nchain);
+        const LigDev L = ligs[lig];
+        const Topo T = topo_view(blobs + L.blob_off);
+        pose_features(T, env, acc + L.best_off + (long long)c * L.stride, nmaps, X + g * mlp::IN);
+    }
+}
+
+__global__ void k_step_advance(int* step_p) { (*step_p)++; }
+
+// rotation vector of the rotation taking the old frame of atoms (f0, f1, f2) to the new one
+__device__ void frame_rotvec(const float* xo, const float* xn, int f0, int f1, int f2, float* rv) {
+    float e[2][3][3];
+    const float* xs[2] = {xo, xn};
+    for (int s = 0; s < 2; s++) {
+        const float* x = xs[s];
+        float u[3], w[3];
+        for (int i = 0; i < 3; i++) { u[i] = x[3 * f1 + i] - x[3 * f0 + i]; w[i] = x[3 * f2 + i] - x[3 * f0 + i]; }
+        const float iu = rsqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        for (int i = 0; i < 3; i++) u[i] *= iu;
+        const float p = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
+        for (int i = 0; i < 3; i++) w[i] -= p * u[i];
+        const float iw = rsqrtf(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        for (int i = 0; i < 3; i++) w[i] *= iw;
+        for (int i = 0; i < 3; i++) { e[s][0][i] = u[i]; e[s][1][i] = w[i]; }
+        e[s][2][0] = u[1] * w[2] - u[2] * w[1];
+        e[s][2][1] = u[2] * w[0] - u[0] * w[2];
+        e[s][2][2] = u[0] * w[1] - u[1] * w[0];
+    }
+    float R[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) R[i][j] = e[1][0][i] * e[0][0][j] + e[1][1][i] * e[0][1][j] + e[1][2][i] * e[0][2][j];
+    const float ct = fminf(fmaxf(0.5f * (R[0][0] + R[1][1] + R[2][2] - 1.f), -1.f), 1.f);
+    const float th = acosf(ct);
+    const float a0 = R[2][1] - R[1][2], a1 = R[0][2] - R[2][0], a2 = R[1][0] - R[0][1];
+    const float sn = sinf(th);
+    const float k = sn > 1e-4f ? th / (2.f * sn) : 0.5f;
+    rv[0] = k * a0; rv[1] = k * a1; rv[2] = k * a2;
+    if (!(rv[0] == rv[0] && rv[1] == rv[1] && rv[2] == rv[2])) rv[0] = rv[1] = rv[2] = 0.f;
+}
+
+// append (features before the move, the move, its mask) to the move set
+__device__ void record_move(const Topo& T, const Env& env, const float* old_rec, Slot P, const __nv_bfloat16* xrow,
+                            MoveSet D) {
+    const int lane = lane_id();
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(D.count, 1);
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= D.max) return;
+    const uint32_t* xs = reinterpret_cast<const uint32_t*>(xrow);
+    uint32_t* xd = reinterpret_cast<uint32_t*>(D.x + (long long)idx * mlp::IN);
+    for (int i = lane; i < mlp::IN / 2; i += WARP) xd[i] = xs[i];
+    float* y = D.y + (long long)idx * mlp::NDIM;
+    float* m = D.m + (long long)idx * mlp::NDIM;
+    const int f0 = T.b[H_FRAME0], f1 = T.b[H_FRAME0 + 1], f2 = T.b[H_FRAME0 + 2];
+    const bool rigid = !env.constraint;
+    if (lane < 3) {
+        y[lane] = P.h[1 + lane] - old_rec[1 + lane];
+        m[lane] = rigid ? 1.f : 0.f;
+    } else if (lane == 3) {
+        float rv[3] = {0.f, 0.f, 0.f};
+        const bool ok = rigid && f0 >= 0;
+        if (ok) frame_rotvec(old_rec + 8, P.x, f0, f1, f2, rv);
+        for (int i = 0; i < 3; i++) { y[3 + i] = rv[i]; m[3 + i] = ok ? 1.f : 0.f; }
+    } else if (lane >= 6 && lane < mlp::NDIM) {
+        const int k = lane - 6;
+        float v = 0.f, mk = 0.f;
+        if (k < T.ntors) {
+            v = normalize_angle(P.d[k] - old_rec[8 + 3 * T.natom + k]);
+            mk = 1.f;
+        }
+        y[lane] = v;
+        m[lane] = mk;
+    }
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_learn_step(const int* __restrict__ blobs,
+                                                        const LigDev* __restrict__ ligs, const int4* __restrict__ items,
+                                                        int nitems, Env env, LearnP sp, const int* __restrict__ step_p,
+                                                        float* acc, float* best, const float* __restrict__ prop_out,
+                                                        const __nv_bfloat16* __restrict__ X, MoveSet rec_set,
+                                                        int* work_counter, unsigned long long* nevals) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ int s_item, s_next, s_lig;
+    int* sblob = reinterpret_cast<int*>(smem);
+    float* wsbase = smem + sp.blob_max;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    float* ws = wsbase + (size_t)warp * sp.ws_max;
+    const int step = *step_p;
+    unsigned long long my_evals = 0, my_heavy = 0;
+    if (threadIdx.x == 0) s_lig = -1;
+    while (true) {
+        if (threadIdx.x == 0) { s_item = atomicAdd(work_counter, 1); s_next = 0; }
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 item = items[it];
+        const LigDev L = ligs[item.x];
+        if (item.x != s_lig)
+            for (int w = threadIdx.x; w < L.stage_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+        __syncthreads();
+        if (threadIdx.x == 0) s_lig = item.x;
+        const Topo T = topo_view(sblob);
+        const int nrec = 8 + 3 * T.natom + T.ntors;
+        const Work W = work_at(ws, T);
+        while (true) {
+            int ci = 0;
+            if (lane == 0) ci = atomicAdd(&s_next, 1);
+            ci = __shfl_sync(FULL, ci, 0);
+            if (ci >= item.z) break;
+            const int c = item.y + ci;
+            const long long g = (long long)item.x * sp.nchain + c;
+            float* out = best + L.best_off + (long long)c * L.stride;
+            float* accp = acc + L.best_off + (long long)c * L.stride;
+            const Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
+            Slot SA = slot_at(ws, L.stride, 0, T.natom);
+            float best_e;
+            if (step == 0) {
+                load_initial(sblob, SA, T.natom, T.ntors);
+                if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
+                best_e = 1e9f;
+            } else {
+                copy_words(SA.h, accp, nrec);
+                best_e = out[0];
+            }
+            __syncwarp();
+            const Proposal prop{(prop_out && step > 0) ? prop_out + g * mlp::OUT : nullptr, sp.p_learned};
+            int ne = 0;
+            bool accepted;
+            const int A = mc_step(T, env, ws, L.stride, 0, W, rng, step, sp.opt_steps, nrec, out, best_e, ne, prop,
+                                  accepted);
+            const Slot SN = slot_at(ws, L.stride, A, T.natom);
+            if (rec_set.count && accepted && step > 0) record_move(T, env, accp, SN, X + g * mlp::IN, rec_set);
+            __syncwarp();
+            copy_words(accp, SN.h, nrec);
             my_evals += ne;
             my_heavy += (unsigned long long)ne * T.nheavy;
         }
@@ -649,6 +903,8 @@ struct LigHost {
 inline int lig_ws(const LigHost& h) { return ws_floats(h.natom, h.ntors, h.nprec); }
 }  // namespace
 
+#include "ud_mlp_host.cuh"
+
 struct ud_ctx {
     int device = 0;
     int nsm = 148;
@@ -689,6 +945,15 @@ struct ud_ctx {
     std::vector<int> h_counts;
     bool has_results = false;
     bool decomp = false;
+    // learned move proposal: the network, the learned search's chain state and step
+    // counter, the features of every chain, and the recorded accepted moves
+    MlpState mlp;
+    DBuf<float> d_acc;
+    DBuf<int> d_step;
+    DBuf<__nv_bfloat16> d_x16, d_mx;
+    DBuf<float> d_my, d_mm;
+    DBuf<int> d_mcount;
+    int moves_max = 0, moves_n = 0;
     // measurement
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     float stage_ms[6] = {0, 0, 0, 0, 0, 0};
@@ -1089,6 +1354,31 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                     blob[o + k] = ent;
                 }
             }
+            {   // rigid frame for recorded moves: three non-collinear atoms of the root fragment
+                std::vector<char> moved(n, 0);
+                for (int q = r0; q < r0 + nrot; q++) moved[rot_atoms[q]] = 1;
+                auto X = [&](int a, int k) { return (double)xyz[3 * (size_t)(a0 + a) + k]; };
+                int f0 = -1, f1 = -1, f2 = -1;
+                for (int i = 0; i < n && f0 < 0; i++) if (!moved[i]) f0 = i;
+                double best = 0.0;
+                for (int i = 0; i < n && f0 >= 0; i++) {
+                    if (moved[i] || i == f0) continue;
+                    double d2 = 0.0;
+                    for (int k = 0; k < 3; k++) d2 += (X(i, k) - X(f0, k)) * (X(i, k) - X(f0, k));
+                    if (d2 > best) { best = d2; f1 = i; }
+                }
+                best = 0.0;
+                for (int i = 0; i < n && f1 >= 0; i++) {
+                    if (moved[i] || i == f0 || i == f1) continue;
+                    double u[3], w[3];
+                    for (int k = 0; k < 3; k++) { u[k] = X(f1, k) - X(f0, k); w[k] = X(i, k) - X(f0, k); }
+                    const double cx = u[1] * w[2] - u[2] * w[1], cy = u[2] * w[0] - u[0] * w[2], cz = u[0] * w[1] - u[1] * w[0];
+                    const double a2 = cx * cx + cy * cy + cz * cz;
+                    if (a2 > best) { best = a2; f2 = i; }
+                }
+                if (f2 < 0 || best < 0.01) f0 = f1 = f2 = -1;       // no rigid frame
+                blob[H_FRAME0] = f0; blob[H_FRAME0 + 1] = f1; blob[H_FRAME0 + 2] = f2;
+            }
             blob[H_TOTAL] = (int)blob.size();
             LigHost h;
             h.natom = n; h.ntors = T; h.nheavy = nheavy;
@@ -1275,60 +1565,78 @@ int ud_bfgs_batch(ud_ctx* c, int n, const int* pose_lig, float* records, int max
     }
 }
 
-static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode) {
-    sync_ligs(c);
-    Env env = make_env(c, mode);
-    int nlig = (int)c->h_ligs.size();
-    c->nchain = nchain;
+// Layout and launch shape of a chain search over the loaded ligands: chain records
+// ligand-major (best_off), warps per CTA and shared memory for the largest ligand, the
+// register budget the shared memory allows, and the work items (ligand, first chain,
+// count) in descending ligand cost, uploaded with the work counter cleared.
+struct SearchPlan {
+    int W = 0, grid = 0, nitems = 0, wsm = 0, blob_max = 0;
+    bool four = false;
+    size_t smem = 0;
     long long tot = 0;
-    int wsm = 0;
+};
+
+extern "C++" {
+template <typename K>
+static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4) {
+    SearchPlan P;
+    const int nlig = (int)c->h_ligs.size();
     std::vector<int> order(nlig);
     std::vector<double> cost(nlig);
     for (int l = 0; l < nlig; l++) {
         const LigHost& h = c->h_ligs[l];
-        c->h_ligdev[l].best_off = tot;
-        tot += (long long)nchain * h.stride;
-        wsm = std::max(wsm, lig_ws(h));
+        c->h_ligdev[l].best_off = P.tot;
+        P.tot += (long long)nchain * h.stride;
+        P.wsm = std::max(P.wsm, lig_ws(h));
         order[l] = l;
         // evaluation cost ~ intra pairs + grid atoms + kinematics, times BFGS length
         const double np = (double)(c->h_blobs[h.blob_off + H_NPAIR]);
         cost[l] = (np + 8.0 * h.natom + 40.0 * h.ntors + 200.0) * (6 + h.ntors);
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    int blob_max = r4(c->max_stage);
-    int W = pick_warps(c, wsm, blob_max, 8);
-    size_t smem = ((size_t)blob_max + (size_t)W * wsm) * 4;
+    P.blob_max = r4(c->max_stage);
+    P.W = pick_warps(c, P.wsm, P.blob_max, 8);
+    P.smem = ((size_t)P.blob_max + (size_t)P.W * P.wsm) * 4;
     int smem_sm = 0;
     ck(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device), "attribute");
     // CTAs per SM the shared memory allows (1 KB per CTA is reserved by the runtime)
-    const bool four = (size_t)smem_sm / (smem + 1024) >= 4;
-    auto kern = four ? k_search<4> : k_search<3>;
-    set_smem(kern, smem);
+    P.four = (size_t)smem_sm / (P.smem + 1024) >= 4;
+    K kern = P.four ? k4 : k3;
+    set_smem(kern, P.smem);
     int per_sm = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * W, smem), "occupancy");
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * P.W, P.smem), "occupancy");
     if (per_sm < 1) per_sm = 1;
     const long long resident = (long long)c->nsm * per_sm;
     // k chains per warp per item (W*k chains): the warps of a CTA share an item's chains
     // dynamically, so the wait at the item's end for its slowest chain shrinks with k;
     // k stays small enough that every resident CTA gets at least two items
     const long long total_chains = (long long)nlig * nchain;
-    const int k = (int)std::max(1LL, std::min(4LL, total_chains / std::max(1LL, 2 * resident * W)));
-    const int item_chains = W * k;
+    const int k = (int)std::max(1LL, std::min(4LL, total_chains / std::max(1LL, 2 * resident * P.W)));
+    const int item_chains = P.W * k;
     std::vector<int4> items;
     for (int l : order)
         for (int c0 = 0; c0 < nchain; c0 += item_chains)
             items.push_back(make_int4(l, c0, std::min(item_chains, nchain - c0), 0));
     upload_ligdev(c);
-    c->best_floats = tot;
-    c->d_best.ensure((size_t)tot);
     c->d_items.upload(items.data(), items.size(), c->stream);
-    const int nitems = (int)items.size();
+    P.nitems = (int)items.size();
+    P.grid = (int)std::min((long long)P.nitems, resident);
     c->d_counter.ensure(1);
     c->d_nevals.ensure(2);
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
     ck(cudaMemsetAsync(c->d_nevals.p, 0, 2 * sizeof(unsigned long long), c->stream), "memset");
-    c->counters[3] = (long long)nlig * nchain;
-    int grid = (int)std::min((long long)nitems, resident);
+    c->counters[3] = total_chains;
+    return P;
+}
+}  // extern "C++"
+
+static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode) {
+    sync_ligs(c);
+    Env env = make_env(c, mode);
+    c->nchain = nchain;
+    const SearchPlan P = plan_search(c, nchain, k_search<3>, k_search<4>);
+    c->best_floats = P.tot;
+    c->d_best.ensure((size_t)P.tot);
     SearchP sp;
     sp.k0 = (uint32_t)seed;
     sp.k1 = (uint32_t)(seed >> 32) ^ 0x5DEECE66u;
@@ -1336,14 +1644,96 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     sp.mc_steps = mc_steps;
     sp.opt_steps = opt_steps;
     sp.randomize = randomize;
-    sp.ws_max = wsm;
-    sp.blob_max = blob_max;
-    if (grid > 0) {
-        kern<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, nitems, env, sp,
-                                                    c->d_best.p, c->d_counter.p, c->d_nevals.p);
+    sp.ws_max = P.wsm;
+    sp.blob_max = P.blob_max;
+    if (P.grid > 0) {
+        auto kern = P.four ? k_search<4> : k_search<3>;
+        kern<<<P.grid, 32 * P.W, P.smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, P.nitems, env, sp,
+                                                      c->d_best.p, c->d_counter.p, c->d_nevals.p);
         ck(cudaGetLastError(), "k_search launch");
         c->counters[2]++;
     }
+}
+
+// The learned-proposal search (and, with record, the collection of accepted moves): one
+// CUDA graph per MC step, replayed mc_steps times.
+static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode,
+                           float p_learned, int record_max) {
+    if (mc_steps < 1) throw Fail(UD_EINVAL, "the learned search needs mc_steps >= 1");
+    if (p_learned < 0.f || p_learned > 1.f) throw Fail(UD_EINVAL, "p_learned must be in [0, 1]");
+    if (p_learned > 0.f && !c->mlp.ready)
+        throw Fail(UD_ESTATE, "no proposal network: call ud_mlp_init, ud_mlp_set_params or train one");
+    if (mode != UD_MODE_GRID) throw Fail(UD_EINVAL, "the learned search scores on the grid maps");
+    sync_ligs(c);
+    Env env = make_env(c, mode);
+    c->nchain = nchain;
+    const int nlig = (int)c->h_ligs.size();
+    const long long nch = (long long)nlig * nchain;
+    for (const LigHost& h : c->h_ligs)
+        if (h.natom > mlp::NATOM || h.ntors > mlp::TMAX)
+            throw Fail(UD_EINVAL, "the proposal network covers ligands of at most 80 atoms and 20 torsions");
+    const SearchPlan P = plan_search(c, nchain, k_learn_step<3>, k_learn_step<4>);
+    c->best_floats = P.tot;
+    c->d_best.ensure((size_t)P.tot);
+    c->d_acc.ensure((size_t)P.tot);
+    const bool feats = p_learned > 0.f || record_max > 0;
+    if (feats) c->d_x16.ensure((size_t)nch * mlp::IN);
+    if (p_learned > 0.f) c->mlp.ensure((int)nch);
+    MoveSet ms{nullptr, nullptr, nullptr, nullptr, 0};
+    if (record_max > 0) {
+        c->d_mx.ensure((size_t)record_max * mlp::IN);
+        c->d_my.ensure((size_t)record_max * mlp::NDIM);
+        c->d_mm.ensure((size_t)record_max * mlp::NDIM);
+        c->d_mcount.ensure(1);
+        ck(cudaMemsetAsync(c->d_mcount.p, 0, sizeof(int), c->stream), "memset");
+        ms = MoveSet{c->d_mx.p, c->d_my.p, c->d_mm.p, c->d_mcount.p, record_max};
+        c->moves_max = record_max;
+    }
+    c->d_step.ensure(1);
+    ck(cudaMemsetAsync(c->d_step.p, 0, sizeof(int), c->stream), "memset");
+    LearnP sp;
+    sp.k0 = (uint32_t)seed;
+    sp.k1 = (uint32_t)(seed >> 32) ^ 0x5DEECE66u;
+    sp.nchain = nchain;
+    sp.opt_steps = opt_steps;
+    sp.randomize = randomize;
+    sp.ws_max = P.wsm;
+    sp.blob_max = P.blob_max;
+    sp.p_learned = p_learned;
+    sp.nfeat_maps = std::min(c->nmaps, mlp::NMAP);
+    auto kern = P.four ? k_learn_step<4> : k_learn_step<3>;
+    const int fblocks = (int)std::min<long long>((nch * 32 + 255) / 256, (long long)c->nsm * 16);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ck(cudaStreamSynchronize(c->stream), "learned search setup");
+    ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
+    try {
+        ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
+        if (feats)
+            k_learn_features<<<fblocks, 256, 0, c->stream>>>(c->d_blobs.p, c->d_ligs.p, nlig, nchain, env, c->d_acc.p,
+                                                             c->d_step.p, sp.nfeat_maps, c->d_x16.p);
+        if (p_learned > 0.f) c->mlp.forward(c->stream, (int)nch, c->d_x16.p);
+        kern<<<P.grid, 32 * P.W, P.smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, P.nitems, env, sp,
+                                                      c->d_step.p, c->d_acc.p, c->d_best.p,
+                                                      p_learned > 0.f ? c->mlp.out.p : nullptr, c->d_x16.p, ms,
+                                                      c->d_counter.p, c->d_nevals.p);
+        k_step_advance<<<1, 1, 0, c->stream>>>(c->d_step.p);
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    ck(cudaStreamEndCapture(c->stream, &graph), "graph capture");
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    ck(ie, "graph instantiate");
+    cudaError_t le = cudaSuccess;
+    for (int s = 0; s < mc_steps && le == cudaSuccess; s++) le = cudaGraphLaunch(exec, c->stream);
+    const cudaError_t se = cudaStreamSynchronize(c->stream);
+    cudaGraphExecDestroy(exec);
+    ck(le, "graph launch");
+    ck(se, "learned search");
+    c->counters[2] += (long long)mc_steps * (3 + (feats ? 1 : 0) + (p_learned > 0.f ? 4 : 0));
 }
 
 static void read_search_counters(ud_ctx* c) {
@@ -1595,6 +1985,222 @@ int ud_sync(ud_ctx* c) {
         if (!c) throw Fail(UD_EINVAL, "null context");
         ck(cudaSetDevice(c->device), "cudaSetDevice");
         ck(cudaStreamSynchronize(c->stream), "sync");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+// ---------------------------------------------------------------------- learned proposal
+long long ud_mlp_param_count(void) { return mlp::NPARAM; }
+
+int ud_mlp_init(ud_ctx* c, uint64_t seed) {
+    try {
+        if (!c) throw Fail(UD_EINVAL, "null context");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        c->mlp.init(seed, c->stream);
+        ck(cudaStreamSynchronize(c->stream), "mlp init");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_mlp_set_params(ud_ctx* c, const float* params) {
+    try {
+        if (!c || !params) throw Fail(UD_EINVAL, "invalid arguments");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        c->mlp.set(params, c->stream);
+        ck(cudaStreamSynchronize(c->stream), "mlp set");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_mlp_get_params(ud_ctx* c, float* params) {
+    try {
+        if (!c || !params) throw Fail(UD_EINVAL, "invalid arguments");
+        if (!c->mlp.ready) throw Fail(UD_ESTATE, "no proposal network: call ud_mlp_init or ud_mlp_set_params");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        ck(cudaMemcpyAsync(params, c->mlp.p.p, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "mlp get");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_mlp_forward(ud_ctx* c, int n, const float* x, float* out) {
+    try {
+        if (!c || n < 0 || (n > 0 && (!x || !out))) throw Fail(UD_EINVAL, "invalid arguments");
+        if (!c->mlp.ready) throw Fail(UD_ESTATE, "no proposal network: call ud_mlp_init or ud_mlp_set_params");
+        if (n == 0) return UD_OK;
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        MlpState& m = c->mlp;
+        m.ensure(n);
+        DBuf<float> dx;
+        dx.upload(x, (size_t)n * mlp::IN, c->stream);
+        k_f32_to_bf16<<<MlpState::blocks((long long)n * mlp::IN), 256, 0, c->stream>>>((long long)n * mlp::IN, dx.p,
+                                                                                        m.x16.p);
+        m.forward(c->stream, n, m.x16.p);
+        ck(cudaMemcpyAsync(out, m.out.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "mlp forward");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_mlp_loss_grad(ud_ctx* c, int n, const float* x, const float* y, const float* mask, double* out_loss,
+                     float* out_grad) {
+    try {
+        if (!c || n <= 0 || !x || !y || !mask || !out_loss || !out_grad) throw Fail(UD_EINVAL, "invalid arguments");
+        if (!c->mlp.ready) throw Fail(UD_ESTATE, "no proposal network: call ud_mlp_init or ud_mlp_set_params");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        MlpState& m = c->mlp;
+        m.ensure(n);
+        DBuf<float> dx, dy, dm;
+        dx.upload(x, (size_t)n * mlp::IN, c->stream);
+        dy.upload(y, (size_t)n * mlp::NDIM, c->stream);
+        dm.upload(mask, (size_t)n * mlp::NDIM, c->stream);
+        k_f32_to_bf16<<<MlpState::blocks((long long)n * mlp::IN), 256, 0, c->stream>>>((long long)n * mlp::IN, dx.p,
+                                                                                        m.x16.p);
+        m.forward(c->stream, n, m.x16.p);
+        m.loss_backward(c->stream, n, m.x16.p, dy.p, dm.p, true);
+        ck(cudaMemcpyAsync(out_loss, m.loss.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaMemcpyAsync(out_grad, m.g.p, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "mlp loss_grad");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+// epochs of minibatch Adam over n device-resident samples (full batches only)
+static void train_on_device(ud_ctx* c, int n, const __nv_bfloat16* x16, const float* y, const float* mk, int epochs,
+                            int batch, float lr, uint64_t seed, float* out_epoch_loss) {
+    cudaStream_t s = c->stream;
+    MlpState& m = c->mlp;
+    const int nb = std::min(batch, n);
+    m.ensure(nb);
+    DBuf<float> by, bm;
+    DBuf<int> didx;
+    by.ensure((size_t)nb * mlp::NDIM);
+    bm.ensure((size_t)nb * mlp::NDIM);
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; i++) perm[i] = i;
+    std::mt19937_64 rng(seed);
+    const int nbatch = n / nb;
+    for (int ep = 0; ep < epochs; ep++) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        didx.upload(perm.data(), (size_t)n, s);
+        for (int b = 0; b < nbatch; b++) {
+            const int* ib = didx.p + (size_t)b * nb;
+            k_gather_rows<<<(int)(((long long)nb * mlp::IN + 255) / 256), 256, 0, s>>>(nb, ib, mlp::IN, x16, m.x16.p);
+            k_gather_rows_f32<<<(nb * mlp::NDIM + 255) / 256, 256, 0, s>>>(nb, ib, mlp::NDIM, y, by.p);
+            k_gather_rows_f32<<<(nb * mlp::NDIM + 255) / 256, 256, 0, s>>>(nb, ib, mlp::NDIM, mk, bm.p);
+            m.forward(s, nb, m.x16.p);
+            m.loss_backward(s, nb, m.x16.p, by.p, bm.p, b == 0);
+            m.adam(s, lr);
+        }
+        double l = 0.0;
+        ck(cudaMemcpyAsync(&l, m.loss.p, sizeof(double), cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "mlp train epoch");
+        if (out_epoch_loss) out_epoch_loss[ep] = (float)(l / std::max(1, nbatch));
+    }
+}
+
+int ud_mlp_train(ud_ctx* c, int n, const float* x, const float* y, const float* mask, int epochs, int batch, float lr,
+                 uint64_t seed, float* out_epoch_loss) {
+    try {
+        if (!c || n <= 0 || !x || !y || !mask || epochs < 0 || batch <= 0) throw Fail(UD_EINVAL, "invalid arguments");
+        if (!c->mlp.ready) throw Fail(UD_ESTATE, "no proposal network: call ud_mlp_init or ud_mlp_set_params");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        cudaStream_t s = c->stream;
+        DBuf<float> dx, dy, dm;
+        DBuf<__nv_bfloat16> x16;
+        dx.upload(x, (size_t)n * mlp::IN, s);
+        x16.ensure((size_t)n * mlp::IN);
+        k_f32_to_bf16<<<MlpState::blocks((long long)n * mlp::IN), 256, 0, s>>>((long long)n * mlp::IN, dx.p, x16.p);
+        ck(cudaStreamSynchronize(s), "mlp train upload");
+        dx.release();
+        dy.upload(y, (size_t)n * mlp::NDIM, s);
+        dm.upload(mask, (size_t)n * mlp::NDIM, s);
+        train_on_device(c, n, x16.p, dy.p, dm.p, epochs, batch, lr, seed, out_epoch_loss);
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_search_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, float p_learned,
+                      long long* out_nevals) {
+    try {
+        if (!c || nchain <= 0 || mc_steps < 1 || opt_steps < 0) throw Fail(UD_EINVAL, "invalid search arguments");
+        if (c->h_ligs.empty()) throw Fail(UD_ESTATE, "no ligands loaded");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        launch_learned(c, seed, nchain, mc_steps, opt_steps, randomize, UD_MODE_GRID, p_learned, 0);
+        read_search_counters(c);
+        c->has_results = false;
+        if (out_nevals) *out_nevals = c->counters[0];
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_collect_moves(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int max_moves,
+                     int* out_count) {
+    try {
+        if (!c || nchain <= 0 || mc_steps < 1 || opt_steps < 0 || max_moves <= 0 || !out_count)
+            throw Fail(UD_EINVAL, "invalid arguments");
+        if (c->h_ligs.empty()) throw Fail(UD_ESTATE, "no ligands loaded");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        launch_learned(c, seed, nchain, mc_steps, opt_steps, randomize, UD_MODE_GRID, 0.f, max_moves);
+        read_search_counters(c);
+        c->has_results = false;
+        int cnt = 0;
+        ck(cudaMemcpyAsync(&cnt, c->d_mcount.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "collect");
+        *out_count = std::min(cnt, max_moves);
+        c->moves_n = *out_count;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_get_moves(ud_ctx* c, int n, float* out_x, float* out_y, float* out_mask) {
+    try {
+        if (!c || n < 0 || n > c->moves_n) throw Fail(UD_EINVAL, "invalid move count");
+        if (n == 0) return UD_OK;
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        if (out_x) {
+            std::vector<uint16_t> h((size_t)n * mlp::IN);
+            ck(cudaMemcpyAsync(h.data(), c->d_mx.p, h.size() * 2, cudaMemcpyDeviceToHost, c->stream), "D2H");
+            ck(cudaStreamSynchronize(c->stream), "moves");
+            for (size_t i = 0; i < h.size(); i++) {
+                const uint32_t u = (uint32_t)h[i] << 16;
+                memcpy(&out_x[i], &u, 4);
+            }
+        }
+        if (out_y) ck(cudaMemcpyAsync(out_y, c->d_my.p, sizeof(float) * n * mlp::NDIM, cudaMemcpyDeviceToHost, c->stream), "D2H");
+        if (out_mask) ck(cudaMemcpyAsync(out_mask, c->d_mm.p, sizeof(float) * n * mlp::NDIM, cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "moves");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_mlp_train_moves(ud_ctx* c, int epochs, int batch, float lr, uint64_t seed, float* out_epoch_loss) {
+    try {
+        if (!c || epochs < 0 || batch <= 0) throw Fail(UD_EINVAL, "invalid arguments");
+        if (c->moves_n <= 0) throw Fail(UD_ESTATE, "no recorded moves: call ud_collect_moves first");
+        if (!c->mlp.ready) throw Fail(UD_ESTATE, "no proposal network: call ud_mlp_init or ud_mlp_set_params");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        train_on_device(c, c->moves_n, c->d_mx.p, c->d_my.p, c->d_mm.p, epochs, batch, lr, seed, out_epoch_loss);
         return UD_OK;
     } catch (const Fail& f) {
         return fail(f);

@@ -1,0 +1,123 @@
+// ud_mlp_host.cuh -- host state of the learned move proposal: device buffers of the
+// network (FP32 master weights, BF16 copy, Adam moments, activations) and the launch
+// sequences of its forward pass, backward pass and Adam step (kernels in ud_mlp.cuh).
+// Included by ud_engine.cu after its device-buffer helpers.
+#pragma once
+#include <random>
+
+struct MlpState {
+    bool ready = false;
+    int adam_t = 0;
+    int cap = 0;
+    DBuf<float> p, g, m, v;                 // NPARAM each
+    DBuf<__nv_bfloat16> p16;
+    DBuf<__nv_bfloat16> x16, h16[3], d16;   // activations of up to cap rows
+    DBuf<float> out, dout, dh, dpre;
+    DBuf<double> loss;
+
+    static int blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 4096); }
+
+    void ensure(int n) {
+        if (n <= cap) return;
+        x16.ensure((size_t)n * mlp::IN);
+        for (auto& h : h16) h.ensure((size_t)n * mlp::HID);
+        d16.ensure((size_t)n * mlp::HID);
+        out.ensure((size_t)n * mlp::OUT);
+        dout.ensure((size_t)n * mlp::OUT);
+        dh.ensure((size_t)n * mlp::HID);
+        dpre.ensure((size_t)n * mlp::HID);
+        cap = n;
+    }
+
+    void init(uint64_t seed, cudaStream_t s) {
+        std::vector<float> h((size_t)mlp::NPARAM, 0.f);
+        std::mt19937_64 rng(seed);
+        auto fill = [&](long long off, int fan_in, long long count) {
+            std::normal_distribution<float> nd(0.f, std::sqrt(2.f / (float)fan_in));
+            for (long long i = 0; i < count; i++) h[(size_t)(off + i)] = nd(rng);
+        };
+        fill(mlp::OFF_W1, mlp::IN, (long long)mlp::IN * mlp::HID);
+        fill(mlp::OFF_W2, mlp::HID, (long long)mlp::HID * mlp::HID);
+        fill(mlp::OFF_W3, mlp::HID, (long long)mlp::HID * mlp::HID);
+        fill(mlp::OFF_W4, mlp::HID, (long long)mlp::HID * mlp::OUT);
+        for (long long i = 0; i < (long long)mlp::HID * mlp::OUT; i++) h[(size_t)(mlp::OFF_W4 + i)] *= 0.1f;
+        set(h.data(), s);
+    }
+
+    void set(const float* host, cudaStream_t s) {
+        p.upload(host, (size_t)mlp::NPARAM, s);
+        g.ensure((size_t)mlp::NPARAM);
+        m.ensure((size_t)mlp::NPARAM);
+        v.ensure((size_t)mlp::NPARAM);
+        p16.ensure((size_t)mlp::NPARAM);
+        ck(cudaMemsetAsync(m.p, 0, sizeof(float) * mlp::NPARAM, s), "memset");
+        ck(cudaMemsetAsync(v.p, 0, sizeof(float) * mlp::NPARAM, s), "memset");
+        k_f32_to_bf16<<<blocks(mlp::NPARAM), 256, 0, s>>>(mlp::NPARAM, p.p, p16.p);
+        ck(cudaGetLastError(), "k_f32_to_bf16");
+        adam_t = 0;
+        ready = true;
+    }
+
+    void gemm(cudaStream_t s, const __nv_bfloat16* A, long long sam, long long sak, const __nv_bfloat16* B,
+              long long sbk, long long sbn, int M, int N, int K, float* C, int ldc, __nv_bfloat16* C16, int ldc16,
+              const float* bias, int relu) {
+        GemmArgs a{A, sam, sak, B, sbk, sbn, M, N, K, C, ldc, C16, ldc16, bias, relu};
+        dim3 grid((N + GBN - 1) / GBN, (M + GBM - 1) / GBM);
+        k_gemm_bf16<<<grid, 128, 0, s>>>(a);
+        ck(cudaGetLastError(), "k_gemm_bf16");
+    }
+
+    // out[n x 64] (FP32) from x16[n x 672]
+    void forward(cudaStream_t s, int n, const __nv_bfloat16* x) {
+        const __nv_bfloat16* w = p16.p;
+        gemm(s, x, mlp::IN, 1, w + mlp::OFF_W1, mlp::HID, 1, n, mlp::HID, mlp::IN, nullptr, 0, h16[0].p, mlp::HID,
+             p.p + mlp::OFF_B1, 1);
+        gemm(s, h16[0].p, mlp::HID, 1, w + mlp::OFF_W2, mlp::HID, 1, n, mlp::HID, mlp::HID, nullptr, 0, h16[1].p,
+             mlp::HID, p.p + mlp::OFF_B2, 1);
+        gemm(s, h16[1].p, mlp::HID, 1, w + mlp::OFF_W3, mlp::HID, 1, n, mlp::HID, mlp::HID, nullptr, 0, h16[2].p,
+             mlp::HID, p.p + mlp::OFF_B3, 1);
+        gemm(s, h16[2].p, mlp::HID, 1, w + mlp::OFF_W4, mlp::OUT, 1, n, mlp::OUT, mlp::HID, out.p, mlp::OUT, nullptr,
+             0, p.p + mlp::OFF_B4, 0);
+    }
+
+    // gradients of the mean NLL into g (after forward on x); the batch's mean loss is
+    // added to loss.p[0] (cleared first when reset)
+    void loss_backward(cudaStream_t s, int n, const __nv_bfloat16* x, const float* Y, const float* M, bool reset) {
+        loss.ensure(1);
+        if (reset) ck(cudaMemsetAsync(loss.p, 0, sizeof(double), s), "memset");
+        const long long no = (long long)n * mlp::OUT;
+        k_mlp_nll<<<(int)((no + 255) / 256), 256, 0, s>>>(n, out.p, Y, M, dout.p, loss.p);
+        ck(cudaGetLastError(), "k_mlp_nll");
+        const __nv_bfloat16* w = p16.p;
+        // output layer: dW4 = h3^T d, db4 = colsum(d), dh3 = d W4^T
+        k_f32_to_bf16<<<blocks(no), 256, 0, s>>>(no, dout.p, d16.p);
+        gemm(s, h16[2].p, 1, mlp::HID, d16.p, mlp::OUT, 1, mlp::HID, mlp::OUT, n, g.p + mlp::OFF_W4, mlp::OUT,
+             nullptr, 0, nullptr, 0);
+        k_colsum<<<1, 64, 0, s>>>(n, mlp::OUT, dout.p, g.p + mlp::OFF_B4);
+        gemm(s, d16.p, mlp::OUT, 1, w + mlp::OFF_W4, 1, mlp::OUT, n, mlp::HID, mlp::OUT, dh.p, mlp::HID, nullptr, 0,
+             nullptr, 0);
+        const long long off_w[3] = {mlp::OFF_W1, mlp::OFF_W2, mlp::OFF_W3};
+        const long long off_b[3] = {mlp::OFF_B1, mlp::OFF_B2, mlp::OFF_B3};
+        const long long nh = (long long)n * mlp::HID;
+        for (int l = 2; l >= 0; l--) {
+            k_relu_bwd<<<blocks(nh), 256, 0, s>>>(nh, dh.p, h16[l].p, dpre.p, d16.p);
+            ck(cudaGetLastError(), "k_relu_bwd");
+            const __nv_bfloat16* hin = l ? h16[l - 1].p : x;
+            const int kin = l ? mlp::HID : mlp::IN;
+            gemm(s, hin, 1, kin, d16.p, mlp::HID, 1, kin, mlp::HID, n, g.p + off_w[l], mlp::HID, nullptr, 0, nullptr,
+                 0);
+            k_colsum<<<1, 256, 0, s>>>(n, mlp::HID, dpre.p, g.p + off_b[l]);
+            if (l > 0)
+                gemm(s, d16.p, mlp::HID, 1, w + off_w[l], 1, mlp::HID, n, mlp::HID, mlp::HID, dh.p, mlp::HID, nullptr,
+                     0, nullptr, 0);
+        }
+        ck(cudaGetLastError(), "mlp backward");
+    }
+
+    void adam(cudaStream_t s, float lr) {
+        adam_t++;
+        const float c1 = 1.f - std::pow(0.9f, (float)adam_t), c2 = 1.f - std::pow(0.999f, (float)adam_t);
+        k_adam<<<blocks(mlp::NPARAM), 256, 0, s>>>(mlp::NPARAM, p.p, g.p, m.p, v.p, p16.p, lr, c1, c2);
+        ck(cudaGetLastError(), "k_adam");
+    }
+};

@@ -76,6 +76,17 @@ def load_library() -> C.CDLL:
         "ud_stream": ([vp], C.c_void_p),
         "ud_stage_times": ([vp, fp], i),
         "ud_counters": ([vp, ip], i),
+        "ud_mlp_param_count": ([], C.c_longlong),
+        "ud_mlp_init": ([vp, C.c_uint64], i),
+        "ud_mlp_set_params": ([vp, fp], i),
+        "ud_mlp_get_params": ([vp, fp], i),
+        "ud_mlp_forward": ([vp, i, fp, fp], i),
+        "ud_mlp_loss_grad": ([vp, i, fp, fp, fp, C.POINTER(C.c_double), fp], i),
+        "ud_mlp_train": ([vp, i, fp, fp, fp, i, i, f, C.c_uint64, fp], i),
+        "ud_search_learned": ([vp, C.c_uint64, i, i, i, i, f, C.POINTER(C.c_longlong)], i),
+        "ud_collect_moves": ([vp, C.c_uint64, i, i, i, i, i, C.POINTER(C.c_int)], i),
+        "ud_get_moves": ([vp, i, fp, fp, fp], i),
+        "ud_mlp_train_moves": ([vp, i, i, f, C.c_uint64, fp], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -273,6 +284,78 @@ class Engine:
                                                   float(vcap), float(slope), _p(e), _p(g)))
         gs = np.split(g, np.cumsum(dims)[:-1]) if len(dims) > 1 else [g]
         return e, gs
+
+    # ------------------------------------------------------------------ learned proposal
+    MLP_IN, MLP_OUT, MLP_NDIM = 672, 64, 26
+
+    def mlp_param_count(self) -> int:
+        return int(self.L.ud_mlp_param_count())
+
+    def mlp_init(self, seed: int = 0):
+        self._check(self.L.ud_mlp_init(self.h, C.c_uint64(seed & (2 ** 64 - 1))))
+
+    def mlp_set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, np.float32)
+        if p.size != self.mlp_param_count():
+            raise EngineError(f"expected {self.mlp_param_count()} parameters, got {p.size}")
+        self._check(self.L.ud_mlp_set_params(self.h, _p(p)))
+
+    def mlp_get_params(self) -> np.ndarray:
+        p = np.zeros(self.mlp_param_count(), np.float32)
+        self._check(self.L.ud_mlp_get_params(self.h, _p(p)))
+        return p
+
+    def mlp_forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.MLP_IN)
+        out = np.zeros((x.shape[0], self.MLP_OUT), np.float32)
+        self._check(self.L.ud_mlp_forward(self.h, x.shape[0], _p(x), _p(out)))
+        return out
+
+    def mlp_loss_grad(self, x, y, mask):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.MLP_IN)
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, self.MLP_NDIM)
+        m = np.ascontiguousarray(mask, np.float32).reshape(-1, self.MLP_NDIM)
+        loss = C.c_double(0.0)
+        g = np.zeros(self.mlp_param_count(), np.float32)
+        self._check(self.L.ud_mlp_loss_grad(self.h, x.shape[0], _p(x), _p(y), _p(m), C.byref(loss), _p(g)))
+        return float(loss.value), g
+
+    def mlp_train(self, x, y, mask, epochs: int, batch: int = 1024, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.MLP_IN)
+        y = np.ascontiguousarray(y, np.float32).reshape(-1, self.MLP_NDIM)
+        m = np.ascontiguousarray(mask, np.float32).reshape(-1, self.MLP_NDIM)
+        losses = np.zeros(max(epochs, 1), np.float32)
+        self._check(self.L.ud_mlp_train(self.h, x.shape[0], _p(x), _p(y), _p(m), int(epochs), int(batch), float(lr),
+                                        C.c_uint64(seed), _p(losses)))
+        return losses[:epochs]
+
+    def search_learned(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, p_learned: float,
+                       randomize: bool = True) -> int:
+        ne = C.c_longlong(0)
+        self._check(self.L.ud_search_learned(self.h, C.c_uint64(seed & (2 ** 64 - 1)), int(nchain), int(mc_steps),
+                                             int(opt_steps), int(randomize), float(p_learned), C.byref(ne)))
+        self.nchain = nchain
+        return int(ne.value)
+
+    def collect_moves(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, max_moves: int,
+                      randomize: bool = True) -> int:
+        n = C.c_int(0)
+        self._check(self.L.ud_collect_moves(self.h, C.c_uint64(seed & (2 ** 64 - 1)), int(nchain), int(mc_steps),
+                                            int(opt_steps), int(randomize), int(max_moves), C.byref(n)))
+        self.nchain = nchain
+        return int(n.value)
+
+    def get_moves(self, n: int):
+        x = np.zeros((n, self.MLP_IN), np.float32)
+        y = np.zeros((n, self.MLP_NDIM), np.float32)
+        m = np.zeros((n, self.MLP_NDIM), np.float32)
+        self._check(self.L.ud_get_moves(self.h, int(n), _p(x), _p(y), _p(m)))
+        return x, y, m
+
+    def mlp_train_moves(self, epochs: int, batch: int = 1024, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        losses = np.zeros(max(epochs, 1), np.float32)
+        self._check(self.L.ud_mlp_train_moves(self.h, int(epochs), int(batch), float(lr), C.c_uint64(seed), _p(losses)))
+        return losses[:epochs]
 
     def score_terms(self, pose_lig, coords, mode: int = MODE_DIRECT, decomp: bool = False):
         pl = np.ascontiguousarray(pose_lig, np.int32)
