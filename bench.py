@@ -1,12 +1,21 @@
-"""Throughput benchmark of the docking engine: ligands/s on the plain virtual-screen workload.
+"""Throughput benchmark of the docking engine on the plain virtual-screen workload:
+ligands/s at a best-score gap of at most 0.3 kcal/mol to the plain 4000-step search for at
+least 95 % of ligands; learned vs plain search.
 
 Workload ("screen"): a 4000-atom synthetic receptor, ligands with 12-48 heavy atoms and
 Poisson(5) rotatable bonds (clipped 0-12), a 30 A box with 0.375 A grid maps (81^3 x types),
-128 MC chains x 4000 steps per ligand with BFGS (opt_steps resolved by the -1 heuristic),
-5 refinement rounds of the cluster leaders, top-9 poses at RMSD 1.0 A, final scoring.
-A step docks one batch of ligands completely.  Inputs are seeded synthetic data.
+128 MC chains per ligand with BFGS (opt_steps resolved by the -1 heuristic), 5 refinement
+rounds of the cluster leaders, top-9 poses at RMSD 1.0 A, final scoring.  A step docks one
+batch of ligands completely.  Inputs are seeded synthetic data.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Default (--mode learned): the plain fused engine docks the batch once at 4000 MC steps (the
+reference result and the plain throughput); a proposal network is trained on the GPU from
+the plain engine's searches of four other seeded ligand sets; the timed steps dock the batch
+with the learned-proposal engine at --learned-steps MC steps.  `value` is the learned
+engine's ligands/s, `quality` the share of ligands whose best score is within 0.3 kcal/mol of
+the 4000-step result.  --mode plain times the fused 4000-step engine instead.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode learned|plain]
 
 N > 1 runs under torchrun, one rank per GPU, each rank docking its own ligands (weak
 scaling, no data-path collective); the timed region is bracketed by a barrier and
@@ -34,7 +43,7 @@ UNIT = "ligands/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="screen")
@@ -44,6 +53,10 @@ def parse():
                     help="MC steps per chain in the untimed warm-up steps (0 = as the timed steps)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--grid", default="f32", choices=["f32", "f16"])
+    ap.add_argument("--mode", default="learned", choices=["learned", "plain"])
+    ap.add_argument("--learned-steps", type=int, default=1000, help="MC steps of the learned-proposal engine")
+    ap.add_argument("--p-learned", type=float, default=0.25, help="share of learned moves")
+    ap.add_argument("--train-ligands", type=int, default=37, help="training ligands per seed (4 seeds)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -210,6 +223,23 @@ def run_reference(a):
     print(json.dumps(out), flush=True)
 
 
+def train_sets(workload: str, n: int, center, seeds=(101, 102, 103, 104)):
+    """Training ligands: four seeded sets of the workload's distribution (not the batch)."""
+    from ud2b200 import synth
+    from ud2b200.model import parse_ligands
+    out = []
+    for sd in seeds:
+        sizes = synth.ligand_sizes(workload, n, sd)
+        d = {f"t{sd}_{i}": synth.make_ligand(na, nt, sd * 7919 + i, center) for i, (na, nt) in enumerate(sizes)}
+        out.append(parse_ligands(d))
+    return out
+
+
+def top_scores(res):
+    """Final score of each ligand's top-ranked pose (intra + inter + penalty + bias)."""
+    return [float(r.terms[0].sum()) if len(r.records) else float("inf") for r in res]
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -229,20 +259,49 @@ def run_ours(a):
     w, box, rec, ligs = make_inputs(a.workload, nl, a.seed, rank)
     mc = a.mc_steps or w["mc_steps"]
     opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
+    learned = a.mode == "learned"
+    tsets = train_sets(a.workload, a.train_ligands, (box.lo.astype(np.float64) + box.hi) / 2.0) if learned else []
+    mt = sorted(set(int(t) for l in list(ligs) + [x for ts in tsets for x in ts] for t in l.types if t != 0))
     eng = Engine(box, device=local)
     eng.set_receptor(rec.xyz, rec.types)
-    mt = sorted(set(int(t) for l in ligs for t in l.types if t != 0))
     eng.build_grid(0.375, mt, GRID_F16 if a.grid == "f16" else GRID_F32)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
-    dock_kw = dict(seed=a.seed, nchain=w["chains"], mc_steps=mc, opt_steps=opt, refine_steps=5,
-                   num_pose=w["num_pose"], rmsd_limit=w["rmsd"], energy_range=10.0, randomize=True, mode=MODE_GRID)
-    # warm-up steps dock the same batch through the same kernels with shorter chains
-    warm_kw = dict(dock_kw, mc_steps=a.warmup_mc_steps or mc)
+    base_kw = dict(seed=a.seed, nchain=w["chains"], opt_steps=opt, refine_steps=5, num_pose=w["num_pose"],
+                   rmsd_limit=w["rmsd"], energy_range=10.0, randomize=True, mode=MODE_GRID)
     from ud2b200.engine import pack_ligands
     packed = pack_ligands(ligs)
     h2d = int(sum(v.nbytes for v in packed.values()))
+    extra = {}
+    if learned:
+        # reference result and plain throughput: the fused engine at the workload's MC steps
+        eng.clear_ligands()
+        eng.add_ligands(ligs)
+        flush.fill_(0.0)
+        torch.cuda.synchronize()
+        res_ref, _ = eng.dock(**base_kw, mc_steps=mc, fetch=True)
+        st = eng.stage_times()
+        ref_scores = np.array(top_scores(res_ref))
+        plain_ms = float(st[5])
+        # proposal network trained on the GPU from the plain engine's own searches
+        from ud2b200.learned import train_proposal
+        params, trep = train_proposal(box, rec, tsets, mt, opt_steps=opt, nchain=w["chains"], mc_steps=150,
+                                      target=1, epochs=6, batch=1024, lr=1e-3, seed=1, device=local)
+        eng.mlp_set_params(params)
+        extra = {"plain": {"value": len(ligs) / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms,
+                           "mc_steps": mc, "engine": "fused plain search (k_search)"},
+                 "learned_training": {"train_ligands": sum(len(t) for t in tsets), "ligand_seeds": [101, 102, 103, 104],
+                                      "samples": trep.samples, "collect_s": trep.collect_s, "train_s": trep.train_s,
+                                      "epoch_loss": trep.epoch_loss, "target": "move to the ligand's best pose"}}
+        run_kw = dict(base_kw, mc_steps=a.learned_steps)
+        p_learned = a.p_learned
+    else:
+        run_kw = dict(base_kw, mc_steps=mc)
+        p_learned = None
+    # warm-up steps dock the same batch through the same kernels with shorter chains
+    warm_kw = dict(run_kw, mc_steps=min(run_kw["mc_steps"], a.warmup_mc_steps or run_kw["mc_steps"]))
     dev_ms, e2e_s, stage, heavy, evals, launches = [], [], [], 0, 0, 0
     sampler = ClockSampler(local)
+    res = None
     for s in range(a.warmup + a.steps):
         if s == a.warmup:
             torch.cuda.synchronize()
@@ -254,7 +313,7 @@ def run_ours(a):
         t0 = time.perf_counter()
         eng.clear_ligands()
         eng.add_ligands(ligs)
-        res, ne = eng.dock(**(dock_kw if s >= a.warmup else warm_kw), fetch=True)
+        res, ne = eng.dock(**(run_kw if s >= a.warmup else warm_kw), fetch=True, p_learned=p_learned)
         t1 = time.perf_counter()
         st = eng.stage_times()
         cn = eng.counters()
@@ -274,6 +333,12 @@ def run_ours(a):
     tot_e2e = sum(e2e_s)
     search_ms = sum(x[0] for x in stage)
     ligs_done = len(ligs) * a.steps
+    if learned:
+        gap = np.array(top_scores(res)) - ref_scores
+        within = float(np.mean(gap <= 0.3))
+        extra["quality"] = {"gap_kcal_mol": 0.3, "within": within, "gate": 0.95, "gate_met": within >= 0.95,
+                            "mean_gap": float(np.mean(gap)), "max_gap": float(np.max(gap)),
+                            "reference": f"plain fused search at {mc} MC steps, same batch, same seed"}
     if dist:
         t = torch.tensor([tot_ms, tot_e2e], dtype=torch.float64, device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -286,18 +351,21 @@ def run_ours(a):
     bytes_alg = heavy * 8 * (2 if a.grid == "f16" else 4)
     achieved = bytes_alg / (search_ms / 1000.0) / 1e9 if search_ms > 0 else 0.0
     tr = load_traffic()
-    traffic = tr if (tr is not None and nl == 148 and mc == w["mc_steps"] and a.workload == "screen") else None
+    traffic = tr if (tr is not None and not learned and nl == 148 and mc == w["mc_steps"] and a.workload == "screen") \
+        else None
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": tot_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic",
-           "config": {"workload": a.workload, "ligands_per_step_per_gpu": len(ligs), "chains": w["chains"],
-                      "mc_steps": mc, "opt_steps": opt, "refine_steps": 5, "num_pose": w["num_pose"],
+           "config": {"workload": a.workload, "engine": "learned proposal" if learned else "fused plain search",
+                      "ligands_per_step_per_gpu": len(ligs), "chains": w["chains"], "mc_steps": run_kw["mc_steps"],
+                      "p_learned": p_learned, "opt_steps": opt, "refine_steps": 5, "num_pose": w["num_pose"],
                       "rmsd_limit": w["rmsd"], "receptor_atoms": rec.natom, "box_A": w["box"], "grid_spacing_A": 0.375,
                       "grid_maps": len(mt), "grid_precision": a.grid, "l2": "flushed between steps (256 MB write)",
                       "warmup": f"{a.warmup} steps, same batch, {warm_kw['mc_steps']} MC steps per chain",
                       "parallelism": f"ligand shards x{world}"},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": traffic, "kernel": "k_search",
+                        "frac": achieved / peak, "traffic": traffic,
+                        "kernel": "k_learn_step" if learned else "k_search",
                         "peak_kind": f"{peak_kind} hbm copy bandwidth",
                         "algorithmic_bytes_per_launch": bytes_alg / a.steps},
            "e2e": {"value": ligs_done / tot_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -306,10 +374,11 @@ def run_ours(a):
            "evaluations_per_step": evals / a.steps,
            "poses_scored_per_s": evals / (search_ms / 1000.0) if search_ms > 0 else None,
            "clocks": sampler.summary()}
+    out.update(extra)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, cores, sample = cpu_port_rate(w, box, rec, ligs, mc, opt, a.cpu_seconds)
         out["cpu_baseline"] = {"value": rate / (w["chains"] * mc), "unit": UNIT, "cores": cores, "kind": "port",
-                               "sample": sample}
+                               "sample": sample + f"; ligands/s at {mc} MC steps per chain"}
     eng.close()
     if rank == 0:
         print(json.dumps(out), flush=True)

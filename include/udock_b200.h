@@ -250,11 +250,16 @@ int ud_mlp_train(ud_ctx* ctx, int n, const float* x, const float* y, const float
 int ud_search_learned(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
                       float p_learned, long long* out_nevals);
 /* Run the plain search (as ud_search_learned with p_learned = 0) and record up to
- * max_moves accepted moves: the features of the pose before the step, the move to the
- * accepted pose (centre shift, rotation vector of a rigid frame of the ligand, wrapped
- * torsion changes) and the mask of the dimensions that apply.  Replaces nothing. */
-int ud_collect_moves(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
+ * max_moves accepted moves: the features of the pose before the step, a move (centre
+ * shift, rotation vector of a rigid frame of the ligand, wrapped torsion changes) and the
+ * mask of the dimensions that apply.  target 0: the move to the accepted pose; target 1:
+ * the move to the best pose of the ligand at the end of the run (over all its chains).
+ * Replaces nothing. */
+int ud_collect_moves(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int target,
                      int max_moves, int* out_count);
+/* ud_dock with the learned-proposal search (ud_search_learned) in place of ud_search;
+ * mode must be UD_MODE_GRID. */
+int ud_dock_learned(ud_ctx* ctx, const ud_dock_params* params, float p_learned, long long* out_nevals);
 /* Copy the first n recorded moves: x[n x 672], y[n x 26], mask[n x 26] (each nullable). */
 int ud_get_moves(ud_ctx* ctx, int n, float* out_x, float* out_y, float* out_mask);
 /* ud_mlp_train on the recorded moves, on the device. */

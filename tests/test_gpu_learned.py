@@ -112,7 +112,7 @@ def test_collect_moves_and_learned_search(search_sys):
     assert 0 < n <= 4000
     x, y, m = eng.get_moves(n)
     assert np.all(np.isfinite(x)) and np.all(np.isfinite(y))
-    assert np.all(np.abs(x) <= 1.0 + 1e-6)                 # squashed features
+    assert np.all(np.abs(x) <= 2.0 + 1e-6)                 # squashed / clamped features
     assert np.all(x[:, 661] == 1.0)
     assert np.all(np.abs(y[:, 6:]) <= np.pi + 1e-5)        # wrapped torsion changes
     ntors = sorted(set(l.ntors for l in ligs))
@@ -130,3 +130,36 @@ def test_collect_moves_and_learned_search(search_sys):
         e = recs[:, 0]
         assert np.all(np.isfinite(e)) and np.all(e < 1e8)
         assert np.all(np.isfinite(recs))
+
+
+def test_collect_moves_to_ligand_best(search_sys):
+    """Target 1: every recorded pose labelled with the move to its ligand's best pose."""
+    eng = search_sys["eng"]
+    ligs = search_sys["ligs"]
+    n = eng.collect_moves(seed=6, nchain=16, mc_steps=8, opt_steps=4, max_moves=2000, target=1)
+    assert n > 0
+    x, y, m = eng.get_moves(n)
+    assert np.all(np.isfinite(y)) and np.all(np.isfinite(x))
+    assert np.all(np.abs(y[:, 6:]) <= np.pi + 1e-5)
+    assert set(np.sum(m[:, 6:], axis=1).astype(int).tolist()) <= set(l.ntors for l in ligs)
+    # the ligand's best pose lies within the 20 A box: centre shifts are bounded by its diagonal
+    assert np.all(np.abs(y[:, :3]) < 40.0)
+
+
+def test_dock_learned_end_to_end(search_sys):
+    """The full dock (search, clustering, refinement, filter, final scores) on the learned
+    search; with p_learned = 0 it returns exactly the fused dock's poses."""
+    eng = search_sys["eng"]
+    kw = dict(seed=3, nchain=16, mc_steps=6, opt_steps=4, refine_steps=2, num_pose=3, rmsd_limit=1.0,
+              energy_range=10.0)
+    eng.mlp_init(4)
+    res, ne = eng.dock(**kw, p_learned=0.5)
+    assert ne > 0 and len(res) == len(search_sys["ligs"])
+    for r in res:
+        assert len(r.records) >= 1 and np.all(np.isfinite(r.terms))
+    a, _ = eng.dock(**kw)
+    b, _ = eng.dock(**kw, p_learned=0.0)
+    for x, y in zip(a, b):
+        assert len(x.records) == len(y.records)
+        for r1, r2 in zip(x.records, y.records):
+            assert np.array_equal(r1, r2)

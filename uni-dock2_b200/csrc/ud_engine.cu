@@ -556,11 +556,16 @@ struct MoveSet {              // recorded accepted moves (training data)
     float* m;                 // [max][26] mask of the dimensions that apply
     int* count;
     int max;
+    int target;               // 0: the move to the next accepted pose; 1: to the ligand's best pose
+    float* aux;               // target 1: [max][32] centre, rigid-frame atoms, dihedrals of the pose
+    long long* chain;         // target 1: [max] chain of the sample
 };
+constexpr int AUX = 32;
 
 // Features of a pose record (672 values): for each of up to 80 atoms the energies of the
 // first 8 grid maps at the atom, squashed v / (1 + |v|); torsion angles / pi; the pose's
-// energy squashed E / (10 + |E|); a constant 1.
+// energy squashed E / (10 + |E|); a constant 1; the centre relative to the box centre in
+// units of 15 A (clamped to +-2); zero padding.
 __device__ void pose_features(const Topo& T, const Env& env, const float* rec, int nmaps, __nv_bfloat16* row) {
     const int lane = lane_id();
     const float* x = rec + 8;
@@ -581,6 +586,11 @@ __device__ void pose_features(const Topo& T, const Env& env, const float* rec, i
         if (k < mlp::TMAX) v = k < T.ntors ? d[k] * (1.f / PI_F) : 0.f;
         else if (k == mlp::TMAX) { const float e = rec[0]; v = __fdividef(e, 10.f + fabsf(e)); if (!(v == v)) v = 0.f; }
         else if (k == mlp::TMAX + 1) v = 1.f;
+        else if (k < mlp::TMAX + 5) {               // centre relative to the box centre / 15 A
+            const int a = k - mlp::TMAX - 2;
+            v = fminf(fmaxf((rec[1 + a] - 0.5f * (env.box_lo[a] + env.box_hi[a])) * (1.f / 15.f), -2.f), 2.f);
+            if (!(v == v)) v = 0.f;
+        }
         row[mlp::NATOM * mlp::NMAP + k] = __float2bfloat16_rn(v);
     }
 }
@@ -603,13 +613,14 @@ __global__ void k_learn_features(const int* __restrict__ blobs, const LigDev* __
 __global__ void k_step_advance(int* step_p) { (*step_p)++; }
 
 // rotation vector of the rotation taking the old frame of atoms (f0, f1, f2) to the new one
-__device__ void frame_rotvec(const float* xo, const float* xn, int f0, int f1, int f2, float* rv) {
+// (po, pn: the frame's three points, 9 floats each, before and after)
+__device__ void frame_rotvec_pts(const float* po, const float* pn, float* rv) {
     float e[2][3][3];
-    const float* xs[2] = {xo, xn};
+    const float* xs[2] = {po, pn};
     for (int s = 0; s < 2; s++) {
         const float* x = xs[s];
         float u[3], w[3];
-        for (int i = 0; i < 3; i++) { u[i] = x[3 * f1 + i] - x[3 * f0 + i]; w[i] = x[3 * f2 + i] - x[3 * f0 + i]; }
+        for (int i = 0; i < 3; i++) { u[i] = x[3 + i] - x[i]; w[i] = x[6 + i] - x[i]; }
         const float iu = rsqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
         for (int i = 0; i < 3; i++) u[i] *= iu;
         const float p = u[0] * w[0] + u[1] * w[1] + u[2] * w[2];
@@ -632,11 +643,58 @@ __device__ void frame_rotvec(const float* xo, const float* xn, int f0, int f1, i
     rv[0] = k * a0; rv[1] = k * a1; rv[2] = k * a2;
     if (!(rv[0] == rv[0] && rv[1] == rv[1] && rv[2] == rv[2])) rv[0] = rv[1] = rv[2] = 0.f;
 }
+__device__ void frame_rotvec(const float* xo, const float* xn, int f0, int f1, int f2, float* rv) {
+    float po[9], pn[9];
+    const int f[3] = {f0, f1, f2};
+    for (int j = 0; j < 3; j++)
+        for (int i = 0; i < 3; i++) { po[3 * j + i] = xo[3 * f[j] + i]; pn[3 * j + i] = xn[3 * f[j] + i]; }
+    frame_rotvec_pts(po, pn, rv);
+}
 
-// append (features before the move, the move, its mask) to the move set
+// append (features before the move, the move, its mask) to the move set; moves with a
+// non-finite value (a chain whose pose diverged) are not recorded
 __device__ void record_move(const Topo& T, const Env& env, const float* old_rec, Slot P, const __nv_bfloat16* xrow,
-                            MoveSet D) {
+                            MoveSet D, long long g) {
     const int lane = lane_id();
+    const int f0 = T.b[H_FRAME0], f1 = T.b[H_FRAME0 + 1], f2 = T.b[H_FRAME0 + 2];
+    if (D.target == 1) {
+        // the pose before the move; its target is labelled after the run (k_label_moves)
+        float a = 0.f;
+        if (lane < 3) a = old_rec[1 + lane];
+        else if (lane < 12) { const int j = (lane - 3) / 3, i = (lane - 3) % 3; const int f = j == 0 ? f0 : (j == 1 ? f1 : f2);
+                              a = f >= 0 ? old_rec[8 + 3 * f + i] : 0.f; }
+        else if (lane - 12 < T.ntors) a = old_rec[8 + 3 * T.natom + (lane - 12)];
+        if (!__all_sync(FULL, isfinite(a))) return;
+        int idx = 0;
+        if (lane == 0) idx = atomicAdd(D.count, 1);
+        idx = __shfl_sync(FULL, idx, 0);
+        if (idx >= D.max) return;
+        const uint32_t* xs = reinterpret_cast<const uint32_t*>(xrow);
+        uint32_t* xd = reinterpret_cast<uint32_t*>(D.x + (long long)idx * mlp::IN);
+        for (int i = lane; i < mlp::IN / 2; i += WARP) xd[i] = xs[i];
+        D.aux[(long long)idx * AUX + lane] = a;
+        if (lane == 0) D.chain[idx] = g;
+        return;
+    }
+    const bool rigid = !env.constraint;
+    float yv = 0.f, mv = 0.f;                 // lane d < 26 holds dimension d
+    float rv[3] = {0.f, 0.f, 0.f};
+    const bool frame_ok = rigid && f0 >= 0;
+    if (lane == 0 && frame_ok) frame_rotvec(old_rec + 8, P.x, f0, f1, f2, rv);
+    rv[0] = __shfl_sync(FULL, rv[0], 0);
+    rv[1] = __shfl_sync(FULL, rv[1], 0);
+    rv[2] = __shfl_sync(FULL, rv[2], 0);
+    if (lane < 3) {
+        yv = P.h[1 + lane] - old_rec[1 + lane];
+        mv = rigid ? 1.f : 0.f;
+    } else if (lane < 6) {
+        yv = rv[lane - 3];
+        mv = frame_ok ? 1.f : 0.f;
+    } else if (lane < mlp::NDIM && lane - 6 < T.ntors) {
+        yv = normalize_angle(P.d[lane - 6] - old_rec[8 + 3 * T.natom + (lane - 6)]);
+        mv = 1.f;
+    }
+    if (!__all_sync(FULL, isfinite(yv))) return;
     int idx = 0;
     if (lane == 0) idx = atomicAdd(D.count, 1);
     idx = __shfl_sync(FULL, idx, 0);
@@ -644,27 +702,77 @@ __device__ void record_move(const Topo& T, const Env& env, const float* old_rec,
     const uint32_t* xs = reinterpret_cast<const uint32_t*>(xrow);
     uint32_t* xd = reinterpret_cast<uint32_t*>(D.x + (long long)idx * mlp::IN);
     for (int i = lane; i < mlp::IN / 2; i += WARP) xd[i] = xs[i];
-    float* y = D.y + (long long)idx * mlp::NDIM;
-    float* m = D.m + (long long)idx * mlp::NDIM;
-    const int f0 = T.b[H_FRAME0], f1 = T.b[H_FRAME0 + 1], f2 = T.b[H_FRAME0 + 2];
-    const bool rigid = !env.constraint;
-    if (lane < 3) {
-        y[lane] = P.h[1 + lane] - old_rec[1 + lane];
-        m[lane] = rigid ? 1.f : 0.f;
-    } else if (lane == 3) {
-        float rv[3] = {0.f, 0.f, 0.f};
-        const bool ok = rigid && f0 >= 0;
-        if (ok) frame_rotvec(old_rec + 8, P.x, f0, f1, f2, rv);
-        for (int i = 0; i < 3; i++) { y[3 + i] = rv[i]; m[3 + i] = ok ? 1.f : 0.f; }
-    } else if (lane >= 6 && lane < mlp::NDIM) {
-        const int k = lane - 6;
-        float v = 0.f, mk = 0.f;
-        if (k < T.ntors) {
-            v = normalize_angle(P.d[k] - old_rec[8 + 3 * T.natom + k]);
-            mk = 1.f;
+    if (lane < mlp::NDIM) {
+        D.y[(long long)idx * mlp::NDIM + lane] = yv;
+        D.m[(long long)idx * mlp::NDIM + lane] = mv;
+    }
+}
+
+// best chain of every ligand (lowest best energy, NaN as +inf, ties to the lower index)
+__global__ void k_lig_best(const LigDev* __restrict__ ligs, int nlig, int nchain, const float* __restrict__ best,
+                           int* out) {
+    __shared__ float se[256];
+    __shared__ int si[256];
+    const int lig = blockIdx.x;
+    if (lig >= nlig) return;
+    const LigDev L = ligs[lig];
+    float e = INFINITY;
+    int ix = 0x7fffffff;
+    for (int c = threadIdx.x; c < nchain; c += blockDim.x) {
+        float v = best[L.best_off + (long long)c * L.stride];
+        if (!(v == v)) v = INFINITY;
+        if (v < e || (v == e && c < ix)) { e = v; ix = c; }
+    }
+    se[threadIdx.x] = e;
+    si[threadIdx.x] = ix;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            const float e2 = se[threadIdx.x + o];
+            const int i2 = si[threadIdx.x + o];
+            if (e2 < se[threadIdx.x] || (e2 == se[threadIdx.x] && i2 < si[threadIdx.x])) { se[threadIdx.x] = e2; si[threadIdx.x] = i2; }
         }
-        y[lane] = v;
-        m[lane] = mk;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[lig] = si[0] == 0x7fffffff ? 0 : si[0];
+}
+
+// targets of recorded poses: the move from each pose to its ligand's best pose
+__global__ void k_label_moves(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int nchain,
+                              const float* __restrict__ best, const int* __restrict__ lig_best, MoveSet D, int n,
+                              int constraint) {
+    const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = lane_id();
+    if (w >= n) return;
+    const long long g = D.chain[w];
+    const int lig = (int)(g / nchain);
+    const LigDev L = ligs[lig];
+    const Topo T = topo_view(blobs + L.blob_off);
+    const float* b = best + L.best_off + (long long)lig_best[lig] * L.stride;
+    const float* a = D.aux + w * AUX;
+    const int f0 = T.b[H_FRAME0], f1 = T.b[H_FRAME0 + 1], f2 = T.b[H_FRAME0 + 2];
+    const bool rigid = !constraint;
+    const bool frame_ok = rigid && f0 >= 0;
+    float rv[3] = {0.f, 0.f, 0.f};
+    if (lane == 0 && frame_ok) {
+        float pn[9];
+        const int f[3] = {f0, f1, f2};
+        for (int j = 0; j < 3; j++)
+            for (int i = 0; i < 3; i++) pn[3 * j + i] = b[8 + 3 * f[j] + i];
+        frame_rotvec_pts(a + 3, pn, rv);
+    }
+    float yv = 0.f, mv = 0.f;
+    const float r0 = __shfl_sync(FULL, rv[0], 0), r1 = __shfl_sync(FULL, rv[1], 0), r2 = __shfl_sync(FULL, rv[2], 0);
+    if (lane < 3) { yv = b[1 + lane] - a[lane]; mv = rigid ? 1.f : 0.f; }
+    else if (lane < 6) { yv = lane == 3 ? r0 : (lane == 4 ? r1 : r2); mv = frame_ok ? 1.f : 0.f; }
+    else if (lane < mlp::NDIM && lane - 6 < T.ntors) {
+        yv = normalize_angle(b[8 + 3 * T.natom + (lane - 6)] - a[12 + (lane - 6)]);
+        mv = 1.f;
+    }
+    if (!isfinite(yv)) { yv = 0.f; mv = 0.f; }
+    if (lane < mlp::NDIM) {
+        D.y[w * mlp::NDIM + lane] = yv;
+        D.m[w * mlp::NDIM + lane] = mv;
     }
 }
 
@@ -725,7 +833,7 @@ __global__ void __launch_bounds__(256, MINB) k_learn_step(const int* __restrict_
             const int A = mc_step(T, env, ws, L.stride, 0, W, rng, step, sp.opt_steps, nrec, out, best_e, ne, prop,
                                   accepted);
             const Slot SN = slot_at(ws, L.stride, A, T.natom);
-            if (rec_set.count && accepted && step > 0) record_move(T, env, accp, SN, X + g * mlp::IN, rec_set);
+            if (rec_set.count && accepted && step > 0) record_move(T, env, accp, SN, X + g * mlp::IN, rec_set, g);
             __syncwarp();
             copy_words(accp, SN.h, nrec);
             my_evals += ne;
@@ -952,7 +1060,9 @@ struct ud_ctx {
     DBuf<int> d_step;
     DBuf<__nv_bfloat16> d_x16, d_mx;
     DBuf<float> d_my, d_mm;
-    DBuf<int> d_mcount;
+    DBuf<int> d_mcount, d_ligbest;
+    DBuf<float> d_maux;
+    DBuf<long long> d_mchain;
     int moves_max = 0, moves_n = 0;
     // measurement
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -1658,7 +1768,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
 // The learned-proposal search (and, with record, the collection of accepted moves): one
 // CUDA graph per MC step, replayed mc_steps times.
 static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode,
-                           float p_learned, int record_max) {
+                           float p_learned, int record_max, int target = 0) {
     if (mc_steps < 1) throw Fail(UD_EINVAL, "the learned search needs mc_steps >= 1");
     if (p_learned < 0.f || p_learned > 1.f) throw Fail(UD_EINVAL, "p_learned must be in [0, 1]");
     if (p_learned > 0.f && !c->mlp.ready)
@@ -1679,14 +1789,19 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     const bool feats = p_learned > 0.f || record_max > 0;
     if (feats) c->d_x16.ensure((size_t)nch * mlp::IN);
     if (p_learned > 0.f) c->mlp.ensure((int)nch);
-    MoveSet ms{nullptr, nullptr, nullptr, nullptr, 0};
+    MoveSet ms{nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr};
     if (record_max > 0) {
         c->d_mx.ensure((size_t)record_max * mlp::IN);
         c->d_my.ensure((size_t)record_max * mlp::NDIM);
         c->d_mm.ensure((size_t)record_max * mlp::NDIM);
         c->d_mcount.ensure(1);
+        if (target == 1) {
+            c->d_maux.ensure((size_t)record_max * AUX);
+            c->d_mchain.ensure((size_t)record_max);
+        }
         ck(cudaMemsetAsync(c->d_mcount.p, 0, sizeof(int), c->stream), "memset");
-        ms = MoveSet{c->d_mx.p, c->d_my.p, c->d_mm.p, c->d_mcount.p, record_max};
+        ms = MoveSet{c->d_mx.p, c->d_my.p, c->d_mm.p, c->d_mcount.p, record_max, target,
+                     target == 1 ? c->d_maux.p : nullptr, target == 1 ? c->d_mchain.p : nullptr};
         c->moves_max = record_max;
     }
     c->d_step.ensure(1);
@@ -1805,7 +1920,9 @@ int ud_cluster(ud_ctx* c, float rmsd_limit, int* out_leaders, int* out_counts) {
     }
 }
 
-int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
+// DockTask::run for the loaded batch; p_learned < 0: the fused search (k_search), else the
+// learned-proposal search with that probability of a learned move
+static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long long* out_nevals) {
     try {
         if (!c || !p || p->nchain <= 0 || p->mc_steps < 0 || p->opt_steps < 0 || p->num_pose <= 0 ||
             p->refine_steps < 0)
@@ -1816,7 +1933,10 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
         c->counters[2] = 0;
         sync_ligs(c);
         c->rec(0);
-        launch_search(c, p->seed, p->nchain, p->mc_steps, p->opt_steps, p->randomize, p->mode);
+        if (p_learned < 0.f)
+            launch_search(c, p->seed, p->nchain, p->mc_steps, p->opt_steps, p->randomize, p->mode);
+        else
+            launch_learned(c, p->seed, p->nchain, p->mc_steps, p->opt_steps, p->randomize, p->mode, p_learned, 0);
         c->rec(1);
         launch_cluster(c, p->rmsd_limit);
         c->counters[2]++;
@@ -1924,6 +2044,16 @@ int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) {
     } catch (const Fail& f) {
         return fail(f);
     }
+}
+
+int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) { return dock_impl(c, p, -1.f, out_nevals); }
+
+int ud_dock_learned(ud_ctx* c, const ud_dock_params* p, float p_learned, long long* out_nevals) {
+    if (!(p_learned >= 0.f && p_learned <= 1.f)) {
+        g_err = "p_learned must be in [0, 1]";
+        return UD_EINVAL;
+    }
+    return dock_impl(c, p, p_learned, out_nevals);
 }
 
 int ud_result_counts(const ud_ctx* c, int* out) {
@@ -2150,14 +2280,15 @@ int ud_search_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int op
     }
 }
 
-int ud_collect_moves(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int max_moves,
-                     int* out_count) {
+int ud_collect_moves(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int target,
+                     int max_moves, int* out_count) {
     try {
-        if (!c || nchain <= 0 || mc_steps < 1 || opt_steps < 0 || max_moves <= 0 || !out_count)
+        if (!c || nchain <= 0 || mc_steps < 1 || opt_steps < 0 || max_moves <= 0 || !out_count ||
+            (target != 0 && target != 1))
             throw Fail(UD_EINVAL, "invalid arguments");
         if (c->h_ligs.empty()) throw Fail(UD_ESTATE, "no ligands loaded");
         ck(cudaSetDevice(c->device), "cudaSetDevice");
-        launch_learned(c, seed, nchain, mc_steps, opt_steps, randomize, UD_MODE_GRID, 0.f, max_moves);
+        launch_learned(c, seed, nchain, mc_steps, opt_steps, randomize, UD_MODE_GRID, 0.f, max_moves, target);
         read_search_counters(c);
         c->has_results = false;
         int cnt = 0;
@@ -2165,6 +2296,17 @@ int ud_collect_moves(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt
         ck(cudaStreamSynchronize(c->stream), "collect");
         *out_count = std::min(cnt, max_moves);
         c->moves_n = *out_count;
+        if (target == 1 && *out_count > 0) {
+            const int nlig = (int)c->h_ligs.size();
+            c->d_ligbest.ensure((size_t)nlig);
+            k_lig_best<<<nlig, 256, 0, c->stream>>>(c->d_ligs.p, nlig, nchain, c->d_best.p, c->d_ligbest.p);
+            MoveSet ms{c->d_mx.p, c->d_my.p, c->d_mm.p, c->d_mcount.p, max_moves, 1, c->d_maux.p, c->d_mchain.p};
+            const long long threads = (long long)*out_count * 32;
+            k_label_moves<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
+                c->d_blobs.p, c->d_ligs.p, nchain, c->d_best.p, c->d_ligbest.p, ms, *out_count, c->constraint);
+            ck(cudaGetLastError(), "label moves");
+            ck(cudaStreamSynchronize(c->stream), "label moves");
+        }
         return UD_OK;
     } catch (const Fail& f) {
         return fail(f);

@@ -84,8 +84,9 @@ def load_library() -> C.CDLL:
         "ud_mlp_loss_grad": ([vp, i, fp, fp, fp, C.POINTER(C.c_double), fp], i),
         "ud_mlp_train": ([vp, i, fp, fp, fp, i, i, f, C.c_uint64, fp], i),
         "ud_search_learned": ([vp, C.c_uint64, i, i, i, i, f, C.POINTER(C.c_longlong)], i),
-        "ud_collect_moves": ([vp, C.c_uint64, i, i, i, i, i, C.POINTER(C.c_int)], i),
+        "ud_collect_moves": ([vp, C.c_uint64, i, i, i, i, i, i, C.POINTER(C.c_int)], i),
         "ud_get_moves": ([vp, i, fp, fp, fp], i),
+        "ud_dock_learned": ([vp, vp, f, C.POINTER(C.c_longlong)], i),
         "ud_mlp_train_moves": ([vp, i, i, f, C.c_uint64, fp], i),
     }
     for name, (args, res) in sig.items():
@@ -338,10 +339,12 @@ class Engine:
         return int(ne.value)
 
     def collect_moves(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, max_moves: int,
-                      randomize: bool = True) -> int:
+                      randomize: bool = True, target: int = 0) -> int:
+        """Record accepted moves of the plain search; target 0: to the next accepted pose,
+        1: to the ligand's best pose at the end of the run."""
         n = C.c_int(0)
         self._check(self.L.ud_collect_moves(self.h, C.c_uint64(seed & (2 ** 64 - 1)), int(nchain), int(mc_steps),
-                                            int(opt_steps), int(randomize), int(max_moves), C.byref(n)))
+                                            int(opt_steps), int(randomize), int(target), int(max_moves), C.byref(n)))
         self.nchain = nchain
         return int(n.value)
 
@@ -403,11 +406,16 @@ class Engine:
     def dock(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, refine_steps: int, num_pose: int,
              rmsd_limit: float, energy_range: float, randomize: bool = True, mode: int = MODE_GRID,
              final_mode: int = MODE_DIRECT, energy_decomp: bool = False,
-             fetch: bool = True) -> Tuple[Optional[List[DockResult]], int]:
+             fetch: bool = True, p_learned: Optional[float] = None) -> Tuple[Optional[List[DockResult]], int]:
+        """Dock the loaded ligands (search, clustering, refinement, filter, final scores);
+        p_learned: None for the fused plain search, else the learned-proposal search."""
         p = DockParams(seed & (2 ** 64 - 1), nchain, mc_steps, opt_steps, refine_steps, num_pose, rmsd_limit,
                        energy_range, int(randomize), mode, final_mode, int(energy_decomp))
         ne = C.c_longlong(0)
-        self._check(self.L.ud_dock(self.h, C.byref(p), C.byref(ne)))
+        if p_learned is None:
+            self._check(self.L.ud_dock(self.h, C.byref(p), C.byref(ne)))
+        else:
+            self._check(self.L.ud_dock_learned(self.h, C.byref(p), float(p_learned), C.byref(ne)))
         self.nchain = nchain
         return (self.results(energy_decomp) if fetch else None), int(ne.value)
 
