@@ -287,11 +287,18 @@ def run_ours(a):
         params, trep = train_proposal(box, rec, tsets, mt, opt_steps=opt, nchain=w["chains"], mc_steps=150,
                                       target=1, epochs=6, batch=1024, lr=1e-3, seed=1, device=local)
         eng.mlp_set_params(params)
+        # the method without the network: the fused plain engine at the learned engine's steps
+        res_eq, _ = eng.dock(**base_kw, mc_steps=a.learned_steps, fetch=True)
+        eq_ms = float(eng.stage_times()[5])
+        gap_eq = np.array(top_scores(res_eq)) - ref_scores
         extra = {"plain": {"value": len(ligs) / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms,
                            "mc_steps": mc, "engine": "fused plain search (k_search)"},
                  "learned_training": {"train_ligands": sum(len(t) for t in tsets), "ligand_seeds": [101, 102, 103, 104],
                                       "samples": trep.samples, "collect_s": trep.collect_s, "train_s": trep.train_s,
-                                      "epoch_loss": trep.epoch_loss, "target": "move to the ligand's best pose"}}
+                                      "epoch_loss": trep.epoch_loss, "target": "move to the ligand's best pose"},
+                 "plain_equal_steps": {"value": len(ligs) / (eq_ms / 1000.0), "unit": UNIT, "mc_steps": a.learned_steps,
+                                       "within": float(np.mean(gap_eq <= 0.3)), "mean_gap": float(np.mean(gap_eq)),
+                                       "engine": "fused plain search at the learned engine's MC steps (untimed)"}}
         run_kw = dict(base_kw, mc_steps=a.learned_steps)
         p_learned = a.p_learned
     else:

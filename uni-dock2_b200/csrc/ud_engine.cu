@@ -379,6 +379,14 @@ __device__ __forceinline__ bool metropolis(float e_old, float e_new, float temp,
 
 __device__ __forceinline__ void store_record(float* dst, Slot P, int nrec) { copy_words(dst, P.h, nrec); }
 
+// a chain's best record before its first improvement: the start pose, energy 1e9 (the
+// bound every chain's first accepted pose is compared against)
+__device__ __forceinline__ void init_best(float* out, Slot P, int nrec) {
+    copy_words(out, P.h, nrec);
+    if (lane_id() == 0) out[0] = 1e9f;
+    __syncwarp();
+}
+
 // A learned move for one MC step: the proposal network's Gaussian (mean, raw log-variance
 // per dimension, 6 + T used) and the probability of taking it instead of a random move.
 struct Proposal {
@@ -414,6 +422,7 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
             float m = prop.out[lane] + __expf(0.5f * lv) * z;
             if (lane < 3) m = fminf(fmaxf(m, -4.f), 4.f);
             else if (lane < 6) m = fminf(fmaxf(m, -PI_F), PI_F);
+            else m = fminf(fmaxf(m, -2.f * PI_F), 2.f * PI_F);
             if (lane < 6 && env.constraint) m = 0.f;
             if (!(m == m)) m = 0.f;
             W.p[lane] = m;
@@ -511,6 +520,7 @@ __global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ bl
             Slot SA = slot_at(ws, L.stride, A, T.natom);
             load_initial(sblob, SA, T.natom, T.ntors);
             if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
+            init_best(out, SA, nrec);
             int ne = 0;
             float best_e = 1e9f;
             if (sp.mc_steps == 0) {
@@ -821,6 +831,7 @@ __global__ void __launch_bounds__(256, MINB) k_learn_step(const int* __restrict_
             if (step == 0) {
                 load_initial(sblob, SA, T.natom, T.ntors);
                 if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
+                init_best(out, SA, nrec);
                 best_e = 1e9f;
             } else {
                 copy_words(SA.h, accp, nrec);
