@@ -223,6 +223,17 @@ def run_reference(a):
     print(json.dumps(out), flush=True)
 
 
+def reduce_over_ranks(dist, dev_ms: float, e2e_s: float, ligs_done: int, device: str):
+    """Whole-job numbers of a multi-rank run: the slowest rank's device and end-to-end
+    times, the ligands of all ranks."""
+    import torch
+    t = torch.tensor([dev_ms, e2e_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    n = torch.tensor([float(ligs_done)], dtype=torch.float64, device=device)
+    dist.all_reduce(n)
+    return float(t[0]), float(t[1]), int(n.item())
+
+
 def train_sets(workload: str, n: int, center, seeds=(101, 102, 103, 104)):
     """Training ligands: four seeded sets of the workload's distribution (not the batch)."""
     from ud2b200 import synth
@@ -263,6 +274,12 @@ def run_ours(a):
     tsets = train_sets(a.workload, a.train_ligands, (box.lo.astype(np.float64) + box.hi) / 2.0) if learned else []
     mt = sorted(set(int(t) for l in list(ligs) + [x for ts in tsets for x in ts] for t in l.types if t != 0))
     eng = Engine(box, device=local)
+    template = a.workload == "template"
+    if template:
+        # template-constrained screen: the shared core stays on its reference pose (no
+        # translation or rotation), every chain keeps 4 poses -> 1024 clustered per ligand
+        eng.set_flags(constraint=True)
+        eng.set_retain(4)
     eng.set_receptor(rec.xyz, rec.types)
     eng.build_grid(0.375, mt, GRID_F16 if a.grid == "f16" else GRID_F32)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
@@ -347,12 +364,7 @@ def run_ours(a):
                             "mean_gap": float(np.mean(gap)), "max_gap": float(np.max(gap)),
                             "reference": f"plain fused search at {mc} MC steps, same batch, same seed"}
     if dist:
-        t = torch.tensor([tot_ms, tot_e2e], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot_ms, tot_e2e = float(t[0]), float(t[1])
-        n = torch.tensor([ligs_done], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(n)
-        ligs_done = int(n.item())
+        tot_ms, tot_e2e, ligs_done = reduce_over_ranks(dist, tot_ms, tot_e2e, ligs_done, f"cuda:{local}")
     value = ligs_done / (tot_ms / 1000.0)
     peak, peak_kind = load_peaks()
     bytes_alg = heavy * 8 * (2 if a.grid == "f16" else 4)
@@ -368,6 +380,7 @@ def run_ours(a):
                       "p_learned": p_learned, "opt_steps": opt, "refine_steps": 5, "num_pose": w["num_pose"],
                       "rmsd_limit": w["rmsd"], "receptor_atoms": rec.natom, "box_A": w["box"], "grid_spacing_A": 0.375,
                       "grid_maps": len(mt), "grid_precision": a.grid, "l2": "flushed between steps (256 MB write)",
+                      "constraint_docking": template, "poses_kept_per_chain": 4 if template else 1,
                       "warmup": f"{a.warmup} steps, same batch, {warm_kw['mc_steps']} MC steps per chain",
                       "parallelism": f"ligand shards x{world}"},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -216,6 +216,20 @@ int ud_stage_times(const ud_ctx* ctx, float* out6);
  * (src/cuda/common.cu:6, src/cuda/mc.cu:443). */
 int ud_counters(const ud_ctx* ctx, long long* out4);
 
+/* Poses kept per chain by ud_search / ud_search_learned / ud_dock (1..4, default 1): each
+ * chain keeps its last `retain` new best poses (its lowest-energy refined poses; records
+ * never filled keep the start pose with energy 1e9); with 1, the reference's one best pose
+ * per chain (src/cuda/mc.cu:389-392).  The chains' moves do not depend on it.  Chain poses,
+ * clustering, refinement and the filter then see nchain * retain poses per ligand, chain
+ * c's at c*retain .. c*retain+retain-1.  No reference counterpart. */
+int ud_set_retain(ud_ctx* ctx, int retain);
+
+/* Chain packing autotuner for ud_search / ud_dock (on != 0): before a batch of a new
+ * shape, times short searches (3 MC steps) with 4 or 8 warps per CTA and 1, 2 or 4 chains
+ * per warp per work item and keeps the fastest.  Results do not depend on the packing.
+ * No reference counterpart (the reference launches one fixed shape, src/cuda/mc.cu:424-440). */
+int ud_set_autotune(ud_ctx* ctx, int on);
+
 /* ---------------------------------------------------------------------------------------
  * Learned move proposal.  No reference counterpart: a BF16 MLP (672 -> 256 -> 256 -> 256
  * -> 64, ReLU, FP32 accumulation on the tensor cores) predicts from a chain's accepted

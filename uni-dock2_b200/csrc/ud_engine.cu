@@ -368,6 +368,7 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
 struct SearchP {
     uint32_t k0, k1;
     int nchain, mc_steps, opt_steps, randomize;
+    int retain;        // poses kept per chain (1..4)
     int ws_max;        // floats per warp
     int blob_max;      // words reserved for the blob
 };
@@ -387,6 +388,49 @@ __device__ __forceinline__ void init_best(float* out, Slot P, int nrec) {
     __syncwarp();
 }
 
+// The poses a chain keeps in records out[r * stride]: its last R (1..4) new best poses,
+// i.e. its R lowest-energy refined poses, each new best replacing the highest kept (1e9
+// marks an unused record).  best() is the bound a refined pose has to beat, so the chain's
+// moves do not depend on R; with R = 1 this is the reference's best pose per chain
+// (mc.cu:376-393).
+// RMAX: 1 (one pose, the common case, no extra registers) or 4 (R <= 4 at run time).
+template <int RMAX>
+struct Retained {
+    float* out;
+    int stride, R;
+    float e0, e1, e2, e3;
+    __device__ __forceinline__ float best() const {
+        if constexpr (RMAX == 1) {
+            return e0;
+        } else {
+            float m = e0;
+            if (R > 1) m = fminf(m, e1);
+            if (R > 2) m = fminf(m, e2);
+            if (R > 3) m = fminf(m, e3);
+            return m;
+        }
+    }
+    __device__ __forceinline__ float worst() const {
+        float m = e0;
+        if (R > 1) m = fmaxf(m, e1);
+        if (R > 2) m = fmaxf(m, e2);
+        if (R > 3) m = fmaxf(m, e3);
+        return m;
+    }
+    __device__ __forceinline__ void store(Slot P, int nrec, float energy) {
+        if constexpr (RMAX == 1) {
+            copy_words(out, P.h, nrec);
+            e0 = energy;
+        } else {
+            const float t = worst();
+            int r = 0;                               // the first record holding the highest energy
+            if (!(e0 == t)) r = (R > 1 && e1 == t) ? 1 : ((R > 2 && e2 == t) ? 2 : 3);
+            copy_words(out + (long long)r * stride, P.h, nrec);
+            if (r == 0) e0 = energy; else if (r == 1) e1 = energy; else if (r == 2) e2 = energy; else e3 = energy;
+        }
+    }
+};
+
 // A learned move for one MC step: the proposal network's Gaussian (mean, raw log-variance
 // per dimension, 6 + T used) and the probability of taking it instead of a random move.
 struct Proposal {
@@ -398,8 +442,9 @@ struct Proposal {
 // with one move applied (a random move, or a sample of the learned proposal), optimised by
 // BFGS with curl 10; Metropolis at T = 1.2 (step 0 always accepts); an accepted new best is
 // optimised again with curl 1000 and recorded.  Returns the accepted slot; sets *accepted.
+template <class Keep>
 __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws, int stride, int A, const Work& W,
-                                       const Rng& rng, int step, int opt_steps, int nrec, float* out, float& best_e,
+                                       const Rng& rng, int step, int opt_steps, int nrec, Keep& keep,
                                        int& ne, const Proposal& prop, bool& accepted) {
     const int lane = lane_id();
     const int C = (A + 1) & 3;
@@ -443,10 +488,7 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
         if (step == 0 || metropolis(e_acc, e, 1.2f, rx)) {
             A = C;
             accepted = true;
-            if (e < best_e) {
-                best_e = e;
-                store_record(out, SC, nrec);
-            }
+            if (e < keep.best()) keep.store(SC, nrec, e);
         }
         return A;
     }
@@ -462,13 +504,10 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
             if (!(step == 0 || metropolis(e_acc, e_new, 1.2f, rx))) break;
             A = R;
             accepted = true;
-            if (!(e_new < best_e)) break;
+            if (!(e_new < keep.best())) break;
         } else {
             A = R;
-            if (e_new < best_e) {
-                best_e = e_new;
-                store_record(out, slot_at(ws, stride, A, T.natom), nrec);
-            }
+            if (e_new < keep.best()) keep.store(slot_at(ws, stride, A, T.natom), nrec, e_new);
         }
     }
     return A;
@@ -480,7 +519,7 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
 // spread over many CTAs and the launch ends with the cheapest items.
 // MINB: 256-thread CTAs per SM the register budget is sized for (4: 64 registers, 3: 80);
 // the host picks the instantiation whose CTA count the shared memory allows.
-template <int MINB>
+template <int MINB, int RMAX>
 __global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ blobs,
                                                 const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                 int nitems, Env env, SearchP sp, float* best, int* work_counter,
@@ -514,15 +553,15 @@ __global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ bl
             ci = __shfl_sync(FULL, ci, 0);
             if (ci >= item.z) break;
             const int c = item.y + ci;
-            float* out = best + L.best_off + (long long)c * L.stride;
+            float* out = best + L.best_off + (long long)c * sp.retain * L.stride;
             Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
             int A = 0;
             Slot SA = slot_at(ws, L.stride, A, T.natom);
             load_initial(sblob, SA, T.natom, T.ntors);
             if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
-            init_best(out, SA, nrec);
+            for (int r = 0; r < sp.retain; r++) init_best(out + (long long)r * L.stride, SA, nrec);
+            Retained<RMAX> keep{out, L.stride, sp.retain, 1e9f, 1e9f, 1e9f, 1e9f};
             int ne = 0;
-            float best_e = 1e9f;
             if (sp.mc_steps == 0) {
                 float e = eval_e_f(T, env, SA.x, W.F, VCAP_SEARCH, PENALTY_SLOPE, W.pb);
                 ne++;
@@ -533,7 +572,7 @@ __global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ bl
                 const Proposal none{nullptr, 0.f};
                 bool acc;
                 for (int step = 0; step < sp.mc_steps; step++)
-                    A = mc_step(T, env, ws, L.stride, A, W, rng, step, sp.opt_steps, nrec, out, best_e, ne, none, acc);
+                    A = mc_step(T, env, ws, L.stride, A, W, rng, step, sp.opt_steps, nrec, keep, ne, none, acc);
             }
             my_evals += ne;
             my_heavy += (unsigned long long)ne * T.nheavy;
@@ -556,6 +595,7 @@ __global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ bl
 struct LearnP {
     uint32_t k0, k1;
     int nchain, opt_steps, randomize;
+    int retain;               // poses kept per chain (1..4)
     int ws_max, blob_max;
     float p_learned;
     int nfeat_maps;           // grid maps used as features (<= 8)
@@ -786,7 +826,7 @@ __global__ void k_label_moves(const int* __restrict__ blobs, const LigDev* __res
     }
 }
 
-template <int MINB>
+template <int MINB, int RMAX>
 __global__ void __launch_bounds__(256, MINB) k_learn_step(const int* __restrict__ blobs,
                                                         const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                         int nitems, Env env, LearnP sp, const int* __restrict__ step_p,
@@ -823,25 +863,27 @@ __global__ void __launch_bounds__(256, MINB) k_learn_step(const int* __restrict_
             if (ci >= item.z) break;
             const int c = item.y + ci;
             const long long g = (long long)item.x * sp.nchain + c;
-            float* out = best + L.best_off + (long long)c * L.stride;
+            float* out = best + L.best_off + (long long)c * sp.retain * L.stride;
             float* accp = acc + L.best_off + (long long)c * L.stride;
             const Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
             Slot SA = slot_at(ws, L.stride, 0, T.natom);
-            float best_e;
+            Retained<RMAX> keep{out, L.stride, sp.retain, 1e9f, 1e9f, 1e9f, 1e9f};
             if (step == 0) {
                 load_initial(sblob, SA, T.natom, T.ntors);
                 if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
-                init_best(out, SA, nrec);
-                best_e = 1e9f;
+                for (int r = 0; r < sp.retain; r++) init_best(out + (long long)r * L.stride, SA, nrec);
             } else {
                 copy_words(SA.h, accp, nrec);
-                best_e = out[0];
+                keep.e0 = out[0];
+                if (sp.retain > 1) keep.e1 = out[L.stride];
+                if (sp.retain > 2) keep.e2 = out[2LL * L.stride];
+                if (sp.retain > 3) keep.e3 = out[3LL * L.stride];
             }
             __syncwarp();
             const Proposal prop{(prop_out && step > 0) ? prop_out + g * mlp::OUT : nullptr, sp.p_learned};
             int ne = 0;
             bool accepted;
-            const int A = mc_step(T, env, ws, L.stride, 0, W, rng, step, sp.opt_steps, nrec, out, best_e, ne, prop,
+            const int A = mc_step(T, env, ws, L.stride, 0, W, rng, step, sp.opt_steps, nrec, keep, ne, prop,
                                   accepted);
             const Slot SN = slot_at(ws, L.stride, A, T.natom);
             if (rec_set.count && accepted && step > 0) record_move(T, env, accp, SN, X + g * mlp::IN, rec_set, g);
@@ -1075,6 +1117,10 @@ struct ud_ctx {
     DBuf<float> d_maux;
     DBuf<long long> d_mchain;
     int moves_max = 0, moves_n = 0;
+    // chain packing autotuner (warps per CTA, chains per warp per work item)
+    int autotune = 0, tune_w = 8, tune_k = 0;
+    int retain = 1;                                   // poses kept per chain
+    long long tune_key = -1;
     // measurement
     cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     float stage_ms[6] = {0, 0, 0, 0, 0, 0};
@@ -1699,7 +1745,7 @@ struct SearchPlan {
 
 extern "C++" {
 template <typename K>
-static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4) {
+static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, int want_w = 8, int force_k = 0) {
     SearchPlan P;
     const int nlig = (int)c->h_ligs.size();
     std::vector<int> order(nlig);
@@ -1707,7 +1753,7 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4) {
     for (int l = 0; l < nlig; l++) {
         const LigHost& h = c->h_ligs[l];
         c->h_ligdev[l].best_off = P.tot;
-        P.tot += (long long)nchain * h.stride;
+        P.tot += (long long)nchain * c->retain * h.stride;
         P.wsm = std::max(P.wsm, lig_ws(h));
         order[l] = l;
         // evaluation cost ~ intra pairs + grid atoms + kinematics, times BFGS length
@@ -1716,7 +1762,7 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4) {
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     P.blob_max = r4(c->max_stage);
-    P.W = pick_warps(c, P.wsm, P.blob_max, 8);
+    P.W = pick_warps(c, P.wsm, P.blob_max, want_w);
     P.smem = ((size_t)P.blob_max + (size_t)P.W * P.wsm) * 4;
     int smem_sm = 0;
     ck(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device), "attribute");
@@ -1732,7 +1778,8 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4) {
     // dynamically, so the wait at the item's end for its slowest chain shrinks with k;
     // k stays small enough that every resident CTA gets at least two items
     const long long total_chains = (long long)nlig * nchain;
-    const int k = (int)std::max(1LL, std::min(4LL, total_chains / std::max(1LL, 2 * resident * P.W)));
+    const int k = force_k > 0 ? force_k
+                              : (int)std::max(1LL, std::min(4LL, total_chains / std::max(1LL, 2 * resident * P.W)));
     const int item_chains = P.W * k;
     std::vector<int4> items;
     for (int l : order)
@@ -1751,13 +1798,8 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4) {
 }
 }  // extern "C++"
 
-static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode) {
-    sync_ligs(c);
-    Env env = make_env(c, mode);
-    c->nchain = nchain;
-    const SearchPlan P = plan_search(c, nchain, k_search<3>, k_search<4>);
-    c->best_floats = P.tot;
-    c->d_best.ensure((size_t)P.tot);
+static void run_search_plan(ud_ctx* c, const SearchPlan& P, const Env& env, uint64_t seed, int nchain, int mc_steps,
+                            int opt_steps, int randomize) {
     SearchP sp;
     sp.k0 = (uint32_t)seed;
     sp.k1 = (uint32_t)(seed >> 32) ^ 0x5DEECE66u;
@@ -1765,15 +1807,63 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     sp.mc_steps = mc_steps;
     sp.opt_steps = opt_steps;
     sp.randomize = randomize;
+    sp.retain = c->retain;
     sp.ws_max = P.wsm;
     sp.blob_max = P.blob_max;
     if (P.grid > 0) {
-        auto kern = P.four ? k_search<4> : k_search<3>;
+        auto kern = c->retain > 1 ? (P.four ? k_search<4, 4> : k_search<3, 4>) : (P.four ? k_search<4, 1> : k_search<3, 1>);
         kern<<<P.grid, 32 * P.W, P.smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, P.nitems, env, sp,
                                                       c->d_best.p, c->d_counter.p, c->d_nevals.p);
         ck(cudaGetLastError(), "k_search launch");
         c->counters[2]++;
     }
+}
+
+// Chain packing autotuner: warps per CTA (4 or 8) and chains per warp per work item
+// (1, 2 or 4), each timed with CUDA events on a short search of the batch itself
+// (3 MC steps); the fastest is kept for batches of the same shape.  A chain's result does
+// not depend on the packing (its random stream is indexed by chain, ligand and step).
+static void autotune_search(ud_ctx* c, const Env& env, uint64_t seed, int nchain, int opt_steps, int randomize) {
+    const long long key = (long long)c->h_ligs.size() * 1000003LL + (long long)nchain * 131LL + c->max_stage * 7LL +
+                          c->retain;
+    if (c->tune_key == key) return;
+    cudaEvent_t e0, e1;
+    ck(cudaEventCreate(&e0), "event");
+    ck(cudaEventCreate(&e1), "event");
+    float best_ms = 1e30f;
+    int best_w = 8, best_k = 0;
+    for (int w : {8, 4})
+        for (int k : {1, 2, 4}) {
+            const SearchPlan P = plan_search(c, nchain, k_search<3, 1>, k_search<4, 1>, w, k);
+            c->d_best.ensure((size_t)P.tot);
+            ck(cudaEventRecord(e0, c->stream), "event");
+            run_search_plan(c, P, env, seed, nchain, 3, opt_steps, randomize);
+            ck(cudaEventRecord(e1, c->stream), "event");
+            ck(cudaEventSynchronize(e1), "autotune");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+            if (ms < best_ms) { best_ms = ms; best_w = w; best_k = k; }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tune_key = key;
+    c->tune_w = best_w;
+    c->tune_k = best_k;
+}
+
+static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode) {
+    sync_ligs(c);
+    Env env = make_env(c, mode);
+    c->nchain = nchain * c->retain;                  // records per ligand
+    if (c->autotune) autotune_search(c, env, seed, nchain, opt_steps, randomize);
+    const SearchPlan P = c->retain > 1
+                             ? (c->autotune ? plan_search(c, nchain, k_search<3, 4>, k_search<4, 4>, c->tune_w, c->tune_k)
+                                            : plan_search(c, nchain, k_search<3, 4>, k_search<4, 4>))
+                             : (c->autotune ? plan_search(c, nchain, k_search<3, 1>, k_search<4, 1>, c->tune_w, c->tune_k)
+                                            : plan_search(c, nchain, k_search<3, 1>, k_search<4, 1>));
+    c->best_floats = P.tot;
+    c->d_best.ensure((size_t)P.tot);
+    run_search_plan(c, P, env, seed, nchain, mc_steps, opt_steps, randomize);
 }
 
 // The learned-proposal search (and, with record, the collection of accepted moves): one
@@ -1787,13 +1877,14 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     if (mode != UD_MODE_GRID) throw Fail(UD_EINVAL, "the learned search scores on the grid maps");
     sync_ligs(c);
     Env env = make_env(c, mode);
-    c->nchain = nchain;
+    c->nchain = nchain * c->retain;                  // records per ligand
     const int nlig = (int)c->h_ligs.size();
     const long long nch = (long long)nlig * nchain;
     for (const LigHost& h : c->h_ligs)
         if (h.natom > mlp::NATOM || h.ntors > mlp::TMAX)
             throw Fail(UD_EINVAL, "the proposal network covers ligands of at most 80 atoms and 20 torsions");
-    const SearchPlan P = plan_search(c, nchain, k_learn_step<3>, k_learn_step<4>);
+    const SearchPlan P = c->retain > 1 ? plan_search(c, nchain, k_learn_step<3, 4>, k_learn_step<4, 4>)
+                                       : plan_search(c, nchain, k_learn_step<3, 1>, k_learn_step<4, 1>);
     c->best_floats = P.tot;
     c->d_best.ensure((size_t)P.tot);
     c->d_acc.ensure((size_t)P.tot);
@@ -1826,8 +1917,10 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     sp.ws_max = P.wsm;
     sp.blob_max = P.blob_max;
     sp.p_learned = p_learned;
+    sp.retain = c->retain;
     sp.nfeat_maps = std::min(c->nmaps, mlp::NMAP);
-    auto kern = P.four ? k_learn_step<4> : k_learn_step<3>;
+    auto kern = c->retain > 1 ? (P.four ? k_learn_step<4, 4> : k_learn_step<3, 4>)
+                              : (P.four ? k_learn_step<4, 1> : k_learn_step<3, 1>);
     const int fblocks = (int)std::min<long long>((nch * 32 + 255) / 256, (long long)c->nsm * 16);
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -1957,7 +2050,8 @@ static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long l
         // from the leader counts
         std::vector<int> counts(nlig);
         ck(cudaMemcpyAsync(counts.data(), c->d_counts.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
-        std::vector<int> leaders((size_t)nlig * p->nchain);
+        const int nrec_lig = c->nchain;                 // records per ligand (chains x retained)
+        std::vector<int> leaders((size_t)nlig * nrec_lig);
         ck(cudaMemcpyAsync(leaders.data(), c->d_leaders.p, leaders.size() * sizeof(int), cudaMemcpyDeviceToHost,
                            c->stream), "D2H");
         ck(cudaStreamSynchronize(c->stream), "search+cluster");
@@ -1970,7 +2064,7 @@ static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long l
                 wsm = std::max(wsm, lig_ws(h));
                 for (int k = 0; k < counts[l]; k++) {
                     il.push_back(l);
-                    io.push_back(c->h_ligdev[l].best_off + (long long)leaders[(size_t)l * p->nchain + k] * h.stride);
+                    io.push_back(c->h_ligdev[l].best_off + (long long)leaders[(size_t)l * nrec_lig + k] * h.stride);
                 }
             }
             int n = (int)il.size();
@@ -2001,9 +2095,9 @@ static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long l
         c->d_sel.ensure((size_t)nlig * p->num_pose);
         c->d_selcnt.ensure(nlig);
         c->d_out.ensure((size_t)of);
-        size_t fsm = (size_t)p->nchain * 8;
+        size_t fsm = (size_t)nrec_lig * 8;
         set_smem(k_filter, fsm);
-        k_filter<<<nlig, 128, fsm, c->stream>>>(c->d_ligs.p, nlig, p->nchain, c->d_best.p, c->d_leaders.p,
+        k_filter<<<nlig, 128, fsm, c->stream>>>(c->d_ligs.p, nlig, nrec_lig, c->d_best.p, c->d_leaders.p,
                                                 c->d_counts.p, p->num_pose, p->energy_range, c->d_sel.p, c->d_selcnt.p);
         ck(cudaGetLastError(), "k_filter launch");
         long long items = (long long)nlig * p->num_pose;
@@ -2130,6 +2224,20 @@ int ud_sync(ud_ctx* c) {
     } catch (const Fail& f) {
         return fail(f);
     }
+}
+
+int ud_set_retain(ud_ctx* c, int retain) {
+    if (!c || retain < 1 || retain > 4) { g_err = "retain must be 1..4"; return UD_EINVAL; }
+    c->retain = retain;
+    c->tune_key = -1;
+    return UD_OK;
+}
+
+int ud_set_autotune(ud_ctx* c, int on) {
+    if (!c) { g_err = "null context"; return UD_EINVAL; }
+    c->autotune = on ? 1 : 0;
+    c->tune_key = -1;
+    return UD_OK;
 }
 
 // ---------------------------------------------------------------------- learned proposal

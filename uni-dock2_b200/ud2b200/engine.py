@@ -76,6 +76,8 @@ def load_library() -> C.CDLL:
         "ud_stream": ([vp], C.c_void_p),
         "ud_stage_times": ([vp, fp], i),
         "ud_counters": ([vp, ip], i),
+        "ud_set_autotune": ([vp, i], i),
+        "ud_set_retain": ([vp, i], i),
         "ud_mlp_param_count": ([], C.c_longlong),
         "ud_mlp_init": ([vp, C.c_uint64], i),
         "ud_mlp_set_params": ([vp, fp], i),
@@ -195,6 +197,7 @@ class Engine:
         self.h = h
         self.ligands: List[Ligand] = []
         self.nchain = 0
+        self.retain = 1
 
     def _check(self, rc: int):
         if rc != 0:
@@ -286,6 +289,15 @@ class Engine:
         gs = np.split(g, np.cumsum(dims)[:-1]) if len(dims) > 1 else [g]
         return e, gs
 
+    def set_retain(self, retain: int):
+        """Poses kept per chain (1..4); chain_poses/cluster then hold nchain * retain poses."""
+        self._check(self.L.ud_set_retain(self.h, int(retain)))
+        self.retain = int(retain)
+
+    def set_autotune(self, on: bool = True):
+        """Time chain packings on each new batch shape and keep the fastest (results unchanged)."""
+        self._check(self.L.ud_set_autotune(self.h, int(bool(on))))
+
     # ------------------------------------------------------------------ learned proposal
     MLP_IN, MLP_OUT, MLP_NDIM = 672, 64, 26
 
@@ -335,7 +347,7 @@ class Engine:
         ne = C.c_longlong(0)
         self._check(self.L.ud_search_learned(self.h, C.c_uint64(seed & (2 ** 64 - 1)), int(nchain), int(mc_steps),
                                              int(opt_steps), int(randomize), float(p_learned), C.byref(ne)))
-        self.nchain = nchain
+        self.nchain = nchain * self.retain
         return int(ne.value)
 
     def collect_moves(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, max_moves: int,
@@ -345,7 +357,7 @@ class Engine:
         n = C.c_int(0)
         self._check(self.L.ud_collect_moves(self.h, C.c_uint64(seed & (2 ** 64 - 1)), int(nchain), int(mc_steps),
                                             int(opt_steps), int(randomize), int(target), int(max_moves), C.byref(n)))
-        self.nchain = nchain
+        self.nchain = nchain * self.retain
         return int(n.value)
 
     def get_moves(self, n: int):
@@ -385,7 +397,7 @@ class Engine:
         ne = C.c_longlong(0)
         self._check(self.L.ud_search(self.h, C.c_uint64(seed & (2 ** 64 - 1)), int(nchain), int(mc_steps),
                                      int(opt_steps), int(randomize), int(mode), C.byref(ne)))
-        self.nchain = nchain
+        self.nchain = nchain * self.retain
         return int(ne.value)
 
     def chain_poses(self, lig: int) -> np.ndarray:
@@ -416,7 +428,7 @@ class Engine:
             self._check(self.L.ud_dock(self.h, C.byref(p), C.byref(ne)))
         else:
             self._check(self.L.ud_dock_learned(self.h, C.byref(p), float(p_learned), C.byref(ne)))
-        self.nchain = nchain
+        self.nchain = nchain * self.retain
         return (self.results(energy_decomp) if fetch else None), int(ne.value)
 
     @property
