@@ -56,6 +56,29 @@ def test_forward_matches_oracle(bare_engine):
     assert np.all(np.abs(got - want) <= 2e-2 + 2e-2 * np.abs(want)), float(np.max(np.abs(got - want)))
 
 
+def test_tcgen05_forward_matches_mma_sync(bare_engine):
+    """The tcgen05 forward pass (tensor-memory accumulator) against the mma.sync one on the
+    same BF16 operands: 300 rows (two full 128-row tiles and a partial one)."""
+    rng = np.random.default_rng(8)
+    p = M.init_params(9)
+    p = (p + rng.normal(0, 0.01, p.size)).astype(np.float32)
+    bare_engine.mlp_set_params(p)
+    X, _, _ = _data(rng, 300)
+    bare_engine.mlp_set_gemm(1)
+    a = bare_engine.mlp_forward(X)
+    bare_engine.mlp_set_gemm(0)
+    try:
+        b = bare_engine.mlp_forward(X)
+    finally:
+        bare_engine.mlp_set_gemm(1)
+    want, _ = M.forward(p, X)
+    d = np.abs(a - b)
+    print(f"tcgen05 vs mma.sync forward: max {d.max():.3e}, median {np.median(d):.3e}")
+    assert np.all(d <= 2e-2 + 2e-2 * np.abs(b))
+    assert float(np.median(d)) <= 1e-3
+    assert np.all(np.abs(a - want) <= 2e-2 + 2e-2 * np.abs(want))
+
+
 def test_loss_and_gradient_match_oracle(bare_engine):
     rng = np.random.default_rng(2)
     p = M.init_params(6)

@@ -1952,6 +1952,7 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     cudaGraphExecDestroy(exec);
     ck(le, "graph launch");
     ck(se, "learned search");
+    if (p_learned > 0.f) c->mlp.check_tc(c->stream);
     c->counters[2] += (long long)mc_steps * (3 + (feats ? 1 : 0) + (p_learned > 0.f ? 4 : 0));
 }
 
@@ -2226,6 +2227,12 @@ int ud_sync(ud_ctx* c) {
     }
 }
 
+int ud_mlp_set_gemm(ud_ctx* c, int kind) {
+    if (!c || (kind != 0 && kind != 1)) { g_err = "kind must be 0 (mma.sync) or 1 (tcgen05)"; return UD_EINVAL; }
+    c->mlp.use_tc = kind == 1;
+    return UD_OK;
+}
+
 int ud_set_retain(ud_ctx* c, int retain) {
     if (!c || retain < 1 || retain > 4) { g_err = "retain must be 1..4"; return UD_EINVAL; }
     c->retain = retain;
@@ -2295,6 +2302,7 @@ int ud_mlp_forward(ud_ctx* c, int n, const float* x, float* out) {
         m.forward(c->stream, n, m.x16.p);
         ck(cudaMemcpyAsync(out, m.out.p, sizeof(float) * n * mlp::OUT, cudaMemcpyDeviceToHost, c->stream), "D2H");
         ck(cudaStreamSynchronize(c->stream), "mlp forward");
+        m.check_tc(c->stream);
         return UD_OK;
     } catch (const Fail& f) {
         return fail(f);
@@ -2320,6 +2328,7 @@ int ud_mlp_loss_grad(ud_ctx* c, int n, const float* x, const float* y, const flo
         ck(cudaMemcpyAsync(out_loss, m.loss.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream), "D2H");
         ck(cudaMemcpyAsync(out_grad, m.g.p, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToHost, c->stream), "D2H");
         ck(cudaStreamSynchronize(c->stream), "mlp loss_grad");
+        m.check_tc(c->stream);
         return UD_OK;
     } catch (const Fail& f) {
         return fail(f);
@@ -2358,6 +2367,7 @@ static void train_on_device(ud_ctx* c, int n, const __nv_bfloat16* x16, const fl
         ck(cudaStreamSynchronize(s), "mlp train epoch");
         if (out_epoch_loss) out_epoch_loss[ep] = (float)(l / std::max(1, nbatch));
     }
+    m.check_tc(s);
 }
 
 int ud_mlp_train(ud_ctx* c, int n, const float* x, const float* y, const float* mask, int epochs, int batch, float lr,

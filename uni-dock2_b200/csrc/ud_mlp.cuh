@@ -122,6 +122,159 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
                 }
 }
 
+// ---------------------------------------------------------------------- tcgen05 forward GEMM
+// Y[M x N] = act(X[M x K] W[K x N] + b) on the 5th-generation tensor cores: one CTA of 128
+// threads per 128-row tile, the FP32 accumulator (128 lanes x N columns) in tensor memory,
+// one thread issuing tcgen05.mma (kind::f16, BF16 operands, M = 128, K = 16 per instruction).
+// Operands are staged 32 K-values at a time, double buffered, in the canonical no-swizzle
+// layouts: X K-major (8 rows x 16 bytes per core matrix), W N-major (8 K-rows x 8 N-values per
+// core matrix), both loaded with 16-byte vector loads.  Each stage's MMAs are committed to
+// that buffer's mbarrier; the buffer is refilled only after its barrier phase completes.
+// Every wait is bounded: on timeout the kernel records an error and skips to the release of
+// its tensor memory.  N is 64 or 256, K a multiple of 32; rows beyond M are zero-filled.
+constexpr int TC_BM = 128, TC_BK = 32;
+constexpr long long TC_SPIN = 1LL << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);        // version 1, no swizzle
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < TC_SPIN; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(bar), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ Wt,
+                                                 const float* __restrict__ bias, int M, int K, int relu,
+                                                 __nv_bfloat16* __restrict__ Y16, float* __restrict__ Y32, int* err) {
+    static_assert(N == 64 || N == 256, "N");
+    constexpr int A_BYTES = TC_BM * TC_BK * 2;              // 8 KB per stage
+    constexpr int B_BYTES = N * TC_BK * 2;                  // 4 or 16 KB per stage
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    unsigned char* sA[2] = {tc_smem, tc_smem + A_BYTES};
+    unsigned char* sB[2] = {tc_smem + 2 * A_BYTES, tc_smem + 2 * A_BYTES + B_BYTES};
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_BM;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&s_tmem)), "r"(N) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_fail = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    // instruction descriptor: F32 accumulate, BF16 A and B, A K-major, B N-major, N, M = 128
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
+                           ((uint32_t)(TC_BM >> 4) << 24);
+    const int nstage = K / TC_BK;
+    const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+    for (int s = 0; s < nstage; s++) {
+        const int b = s & 1;
+        if (s >= 2) {
+            if (!mbar_wait(smem_u32(&bars[b]), (uint32_t)(((s - 2) >> 1) & 1))) { if (tid == 0) s_fail = 1; }
+            __syncthreads();
+            if (s_fail) break;
+        }
+        const int k0 = s * TC_BK;
+        // X tile: row m, 8 consecutive k per 16-byte vector; K-major core matrices
+        for (int v = tid; v < TC_BM * (TC_BK / 8); v += 128) {
+            const int r = v >> 2, kc = v & 3;                  // kc: 8-wide k chunk 0..3
+            const int m = m0 + r;
+            const uint4 val = m < M ? *reinterpret_cast<const uint4*>(X + (long long)m * K + k0 + kc * 8) : zero4;
+            const int step = kc >> 1, half = kc & 1;
+            *reinterpret_cast<uint4*>(sA[b] + step * (TC_BM / 8) * 256 + (r >> 3) * 256 + half * 128 + (r & 7) * 16) = val;
+        }
+        // W tile: k row, 8 consecutive n per 16-byte vector; N-major core matrices
+        for (int v = tid; v < TC_BK * (N / 8); v += 128) {
+            const int kk = v / (N / 8), nc = v % (N / 8);
+            const uint4 val = *reinterpret_cast<const uint4*>(Wt + (long long)(k0 + kk) * N + nc * 8);
+            const int step = kk >> 4, kg = (kk >> 3) & 1, kr = kk & 7;
+            *reinterpret_cast<uint4*>(sB[b] + step * (N / 8) * 256 + kg * (N / 8) * 128 + nc * 128 + kr * 16) = val;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int step = 0; step < TC_BK / 16; step++) {
+                const uint64_t da = umma_desc(smem_u32(sA[b] + step * (TC_BM / 8) * 256), 128, 256);
+                const uint64_t db = umma_desc(smem_u32(sB[b] + step * (N / 8) * 256), (N / 8) * 128, 128);
+                const uint32_t acc = (s > 0 || step > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+                    :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         :: "r"(smem_u32(&bars[b])) : "memory");
+        }
+    }
+    // all MMAs done when the last stage's barrier phase completes
+    if (!s_fail && nstage > 0) {
+        const int last = nstage - 1;
+        if (!mbar_wait(smem_u32(&bars[last & 1]), (uint32_t)((last >> 1) & 1))) { if (tid == 0) s_fail = 1; }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!s_fail) {
+        const int m = m0 + warp * 32 + lane;                   // this thread's row (TMEM lane)
+        for (int c = 0; c < N; c += 8) {
+            uint32_t r[8];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < M) {
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    v[j] = __uint_as_float(r[j]) + (bias ? bias[c + j] : 0.f);
+                    if (relu) v[j] = fmaxf(v[j], 0.f);
+                }
+                if (Y32) {
+#pragma unroll
+                    for (int j = 0; j < 8; j++) Y32[(long long)m * N + c + j] = v[j];
+                }
+                if (Y16) {
+                    __nv_bfloat162 h[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) h[j] = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+                    *reinterpret_cast<uint4*>(Y16 + (long long)m * N + c) = *reinterpret_cast<uint4*>(h);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, 1);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(N) : "memory");
+}
+
 __global__ void k_f32_to_bf16(long long n, const float* __restrict__ s, __nv_bfloat16* __restrict__ d) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         d[i] = __float2bfloat16_rn(s[i]);

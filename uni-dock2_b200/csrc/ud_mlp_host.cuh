@@ -9,6 +9,9 @@ struct MlpState {
     bool ready = false;
     int adam_t = 0;
     int cap = 0;
+    bool use_tc = true;                     // forward pass on tcgen05 (else mma.sync)
+    bool tc_attr = false;
+    DBuf<int> tc_err;                       // set by a tcgen05 GEMM whose wait timed out
     DBuf<float> p, g, m, v;                 // NPARAM each
     DBuf<__nv_bfloat16> p16;
     DBuf<__nv_bfloat16> x16, h16[3], d16;   // activations of up to cap rows
@@ -67,8 +70,47 @@ struct MlpState {
         ck(cudaGetLastError(), "k_gemm_bf16");
     }
 
+    static constexpr int TC_SMEM = 96 * 1024;   // more than the 48 KB of stages: at most 2 CTAs
+                                                // per SM, so 2 x 256 tensor-memory columns fit
+
+    void tc_layer(cudaStream_t s, int n, const __nv_bfloat16* x, int K, long long off_w, long long off_b, int N,
+                  int relu, __nv_bfloat16* y16, float* y32) {
+        const unsigned grid = (unsigned)((n + TC_BM - 1) / TC_BM);
+        if (N == 256)
+            k_gemm_tc<256><<<grid, 128, TC_SMEM, s>>>(x, p16.p + off_w, p.p + off_b, n, K, relu, y16, y32, tc_err.p);
+        else
+            k_gemm_tc<64><<<grid, 128, TC_SMEM, s>>>(x, p16.p + off_w, p.p + off_b, n, K, relu, y16, y32, tc_err.p);
+        ck(cudaGetLastError(), "k_gemm_tc");
+    }
+
+    // errors recorded by the tensor-core GEMM since the last check (call after a sync)
+    void check_tc(cudaStream_t s) {
+        if (!tc_err.p) return;
+        int e = 0;
+        ck(cudaMemcpyAsync(&e, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+        ck(cudaStreamSynchronize(s), "tensor-core GEMM check");
+        if (e) {
+            ck(cudaMemsetAsync(tc_err.p, 0, sizeof(int), s), "memset");
+            throw Fail(UD_ECUDA, "tensor-core GEMM: a wait for its MMAs timed out");
+        }
+    }
+
     // out[n x 64] (FP32) from x16[n x 672]
     void forward(cudaStream_t s, int n, const __nv_bfloat16* x) {
+        if (use_tc) {
+            if (!tc_attr) {
+                ck(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
+                ck(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
+                tc_err.ensure(1);
+                ck(cudaMemsetAsync(tc_err.p, 0, sizeof(int), s), "memset");
+                tc_attr = true;
+            }
+            tc_layer(s, n, x, mlp::IN, mlp::OFF_W1, mlp::OFF_B1, mlp::HID, 1, h16[0].p, nullptr);
+            tc_layer(s, n, h16[0].p, mlp::HID, mlp::OFF_W2, mlp::OFF_B2, mlp::HID, 1, h16[1].p, nullptr);
+            tc_layer(s, n, h16[1].p, mlp::HID, mlp::OFF_W3, mlp::OFF_B3, mlp::HID, 1, h16[2].p, nullptr);
+            tc_layer(s, n, h16[2].p, mlp::HID, mlp::OFF_W4, mlp::OFF_B4, mlp::OUT, 0, nullptr, out.p);
+            return;
+        }
         const __nv_bfloat16* w = p16.p;
         gemm(s, x, mlp::IN, 1, w + mlp::OFF_W1, mlp::HID, 1, n, mlp::HID, mlp::IN, nullptr, 0, h16[0].p, mlp::HID,
              p.p + mlp::OFF_B1, 1);

@@ -80,6 +80,7 @@ def load_library() -> C.CDLL:
         "ud_set_retain": ([vp, i], i),
         "ud_mlp_param_count": ([], C.c_longlong),
         "ud_mlp_init": ([vp, C.c_uint64], i),
+        "ud_mlp_set_gemm": ([vp, i], i),
         "ud_mlp_set_params": ([vp, fp], i),
         "ud_mlp_get_params": ([vp, fp], i),
         "ud_mlp_forward": ([vp, i, fp, fp], i),
@@ -303,6 +304,10 @@ class Engine:
 
     def mlp_param_count(self) -> int:
         return int(self.L.ud_mlp_param_count())
+
+    def mlp_set_gemm(self, kind: int):
+        """Forward pass on tcgen05 (1, default) or mma.sync (0)."""
+        self._check(self.L.ud_mlp_set_gemm(self.h, int(kind)))
 
     def mlp_init(self, seed: int = 0):
         self._check(self.L.ud_mlp_init(self.h, C.c_uint64(seed & (2 ** 64 - 1))))
