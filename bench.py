@@ -192,6 +192,43 @@ def cpu_port_rate(w, box, rec, ligs, mc_steps, opt_steps, seconds: float, mode: 
                         f"{mode} scoring, in {el:.1f} s"
 
 
+def reference_scoring_rate(rec, box, ligs, seconds: float = 8.0):
+    """Poses scored per second by the reference's own host score() (src/score/score.cpp,
+    compiled from the reference sources into oracle/_ref, OpenMP over poses on all host
+    cores): energy of rigidly placed copies of the batch's first ligand.  None when that
+    library was not built."""
+    import ctypes as C
+    import numpy as np
+    path = os.path.join(ROOT, "oracle", "_ref", "libudref_f32.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    lig = ligs[0]
+    rng = np.random.default_rng(5)
+    npose = 2048
+    mid = ((box.lo + box.hi) / 2.0).astype(np.float32)
+    base = (lig.coords - lig.coords.mean(axis=0)).astype(np.float32)
+    xs = np.ascontiguousarray(np.stack([base + mid + rng.uniform(-3, 3, 3).astype(np.float32) for _ in range(npose)]),
+                              np.float32)
+    types = np.ascontiguousarray(lig.types, np.int32)
+    off = np.ascontiguousarray(lig.pair_off, np.int32)
+    pairs = np.ascontiguousarray(lig.pairs, np.int32)
+    rxyz = np.ascontiguousarray(rec.xyz, np.float32)
+    rt = np.ascontiguousarray(rec.types, np.int32)
+    box6 = np.ascontiguousarray(box.as6(), np.float32)
+    out = np.zeros((npose, 4), np.float32)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        L.udref_score_batch(C.c_int(npose), C.c_int(lig.natom), p(xs), p(types), p(off), p(pairs), C.c_int(rec.natom),
+                            p(rxyz), p(rt), p(box6), p(out))
+        done += npose
+    el = time.perf_counter() - t0
+    return {"value": done / el, "unit": "poses/s", "cores": os.cpu_count() or 1, "kind": "reference",
+            "sample": f"{done} poses of a {lig.natom}-atom screen ligand against {rec.natom} receptor atoms, "
+                      f"the reference's score() (energy only, direct pair sum), OpenMP over poses, {el:.1f} s"}
+
+
 # ------------------------------------------------------------------------- main arms
 def run_reference(a):
     """The reference's CPU path on this host: the oracle restatement of the reference's
@@ -220,6 +257,9 @@ def run_reference(a):
                       "receptor_atoms": rec.natom, "box_A": w["box"]},
            "cpu_baseline": {"value": lig_s, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": lig_s, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    ref_sc = reference_scoring_rate(rec, box, ligs)
+    if ref_sc:
+        out["reference_cpu_scoring"] = ref_sc
     print(json.dumps(out), flush=True)
 
 
@@ -399,6 +439,9 @@ def run_ours(a):
         rate, cores, sample = cpu_port_rate(w, box, rec, ligs, mc, opt, a.cpu_seconds)
         out["cpu_baseline"] = {"value": rate / (w["chains"] * mc), "unit": UNIT, "cores": cores, "kind": "port",
                                "sample": sample + f"; ligands/s at {mc} MC steps per chain"}
+        ref_sc = reference_scoring_rate(rec, box, ligs)
+        if ref_sc:
+            out["reference_cpu_scoring"] = ref_sc
     eng.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
