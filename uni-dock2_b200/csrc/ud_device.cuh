@@ -256,6 +256,15 @@ __device__ __forceinline__ float warp_sum(float v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
     return v;
 }
+// three warp sums at once: the same butterfly per value (bit-identical to three warp_sum
+// calls), interleaved so that their shuffle latencies overlap
+__device__ __forceinline__ void warp_sum3(float& a, float& b, float& c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ta = __shfl_xor_sync(FULL, a, o), tb = __shfl_xor_sync(FULL, b, o), tc = __shfl_xor_sync(FULL, c, o);
+        a += ta; b += tb; c += tc;
+    }
+}
 
 // Reduce-scatter of 16 per-lane values: after the call, a[0] of lane L holds the warp
 // total of value v = bit4(L)<<3 | bit3(L)<<2 | bit2(L)<<1 | bit1(L).  16 shuffles
@@ -745,7 +754,7 @@ __device__ __forceinline__ void refresh_center(const Topo& T, Slot P) {
     const int lane = lane_id();
     float s0 = 0.f, s1 = 0.f, s2 = 0.f;
     for (int i = lane; i < T.natom; i += WARP) { s0 += P.x[3 * i]; s1 += P.x[3 * i + 1]; s2 += P.x[3 * i + 2]; }
-    s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2);
+    warp_sum3(s0, s1, s2);
     __syncwarp();
     if (lane == 0) {
         const float n = (float)T.natom;
@@ -908,23 +917,27 @@ __device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots,
         float alpha;
         const float E1 = line_search(T, env, slot_at(slots, stride, cur, T.natom),
                                      slot_at(slots, stride, alt, T.natom), W, dim, E, vcap, slope, alpha, n_eval);
-        for (int i = lane; i < dim; i += WARP) W.y[i] = W.gn[i] - W.g[i];
+        // y = g_new - g with g.g (the reference tests the old gradient), y.p and y.y in one
+        // reduction (each the same sum as a separate dot product)
+        float gg = 0.f, yp = 0.f, yy = 0.f;
+        for (int i = lane; i < dim; i += WARP) {
+            const float gi = W.g[i], yi = W.gn[i] - gi;
+            W.y[i] = yi;
+            gg += gi * gi;
+            yp += yi * W.p[i];
+            yy += yi * yi;
+        }
+        warp_sum3(gg, yp, yy);
         __syncwarp();
         E = E1;
         const int t = cur; cur = alt; alt = t;                // x := x_new
-        const float gg = gdot(W.g, W.g, dim);                 // the reference tests the old gradient
         if (sqrtf(gg) < 1e-5f) break;
         for (int i = lane; i < dim; i += WARP) W.g[i] = W.gn[i];
         __syncwarp();
-        if (step == 0) {
-            const float yy = gdot(W.y, W.y, dim);
-            if (fabsf(yy) > EPS_F) {
-                const float yp0 = gdot(W.y, W.p, dim);
-                for (int i = lane; i < dim; i += WARP) W.H[i + i * (i + 1) / 2] = (double)(alpha * yp0 / yy);
-                __syncwarp();
-            }
+        if (step == 0 && fabsf(yy) > EPS_F) {
+            for (int i = lane; i < dim; i += WARP) W.H[i + i * (i + 1) / 2] = (double)(alpha * yp / yy);
+            __syncwarp();
         }
-        const float yp = gdot(W.y, W.p, dim);
         if (alpha * yp < EPS_F) continue;
         minus_hv(W.H, W.y, W.mhy, dim);
         const double yhy = -(double)gdot(W.y, W.mhy, dim);
