@@ -162,7 +162,9 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
     static_assert(N == 64 || N == 256, "N");
     constexpr int A_BYTES = TC_BM * TC_BK * 2;              // 8 KB per stage
     constexpr int B_BYTES = N * TC_BK * 2;                  // 4 or 16 KB per stage
-    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    extern __shared__ __align__(16) unsigned char tc_smem_raw[];
+    // operand stages from a 1024-byte boundary (the launch requests 1 KB of slack)
+    unsigned char* tc_smem = tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u);
     unsigned char* sA[2] = {tc_smem, tc_smem + A_BYTES};
     unsigned char* sB[2] = {tc_smem + 2 * A_BYTES, tc_smem + 2 * A_BYTES + B_BYTES};
     __shared__ __align__(8) uint64_t bars[2];
