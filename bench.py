@@ -45,7 +45,9 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--ref-ligands", type=int, default=8, help="ligands of the reference-gpu comparison")
+    ap.add_argument("--ref-mc-steps", type=int, default=200, help="MC steps of the reference-gpu comparison")
     ap.add_argument("--workload", default="screen")
     ap.add_argument("--ligands", type=int, default=148, help="ligands per step per GPU")
     ap.add_argument("--mc-steps", type=int, default=0, help="override MC steps (0 = workload value)")
@@ -291,6 +293,61 @@ def top_scores(res):
     return [float(r.terms[0].sum()) if len(r.records) else float("inf") for r in res]
 
 
+def run_reference_gpu(a):
+    """The reference's own CUDA engine (core_pipeline, built from its sources into
+    oracle/_ref/udref_dock) and this engine on the same small batch and settings, both on
+    this GPU; ligands/s are extrapolated to the workload's MC steps (the time is linear in
+    MC steps).  Run on demand only."""
+    import tempfile
+    import numpy as np
+    from ud2b200 import synth, Engine, MODE_GRID
+    from ud2b200.batching import heuristic_opt_steps
+    from ud2b200.model import Box, parse_ligands, parse_receptor
+    exe = os.path.join(ROOT, "oracle", "_ref", "udref_dock")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/udref_dock not built (make -C oracle refengine)"}))
+        return
+    w = synth.WORKLOADS[a.workload]
+    rows, center = synth.make_receptor(w["nrec"], w["cube"], a.seed)
+    box = Box.from_center_size(center, [w["box"]] * 3)
+    sizes = synth.ligand_sizes(a.workload, a.ref_ligands, a.seed)
+    ligd = {f"lig{i:04d}": synth.make_ligand(n, t, a.seed * 7919 + i, center) for i, (n, t) in enumerate(sizes)}
+    ligs = parse_ligands(ligd)
+    opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
+    steps = a.ref_mc_steps
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "input.json")
+        with open(inp, "w") as f:
+            json.dump(dict(receptor=rows, **ligd), f)
+        cmd = [exe, inp, os.path.join(tmp, "out"), *[str(float(v)) for v in center], *[str(float(w["box"]))] * 3,
+               str(w["chains"]), str(steps), str(opt), "5", str(w["num_pose"]), str(w["rmsd"]), "10.0", str(a.seed), "0"]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600)
+        line = [l for l in r.stdout.splitlines() if l.startswith("{")]
+        ref = json.loads(line[-1]) if line else {"rc": r.returncode}
+    rec = parse_receptor(rows, box)
+    eng = Engine(box)
+    eng.set_receptor(rec.xyz, rec.types)
+    mt = sorted(set(int(t) for l in ligs for t in l.types if t != 0))
+    t0 = time.perf_counter()
+    eng.build_grid(0.375, mt)
+    eng.add_ligands(ligs)
+    res, _ = eng.dock(seed=a.seed, nchain=w["chains"], mc_steps=steps, opt_steps=opt, refine_steps=5,
+                      num_pose=w["num_pose"], rmsd_limit=w["rmsd"], energy_range=10.0, fetch=True)
+    ours_s = time.perf_counter() - t0
+    eng.close()
+    full = w["mc_steps"] / steps
+    out = {"impl": "reference-gpu", "metric": METRIC, "unit": UNIT, "workload": a.workload, "ligands": len(ligs),
+           "chains": w["chains"], "mc_steps_run": steps, "mc_steps_workload": w["mc_steps"], "opt_steps": opt,
+           "reference": {"rc": ref.get("rc"), "seconds": ref.get("seconds"),
+                         "value": (len(ligs) / (ref["seconds"] * full)) if ref.get("seconds") else None,
+                         "engine": "the reference's core_pipeline (direct pair sums), built from its sources"},
+           "ours": {"seconds": ours_s, "value": len(ligs) / (ours_s * full),
+                    "engine": "this engine, ud_dock with grid maps (grid build included)"},
+           "note": "wall times of one call each on the same GPU and inputs; ligands/s extrapolated linearly "
+                   f"from {steps} to {w['mc_steps']} MC steps"}
+    print(json.dumps(out), flush=True)
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -454,6 +511,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.impl == "reference-gpu":
+        run_reference_gpu(a)
     else:
         run_ours(a)
 
