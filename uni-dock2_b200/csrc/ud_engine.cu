@@ -1890,7 +1890,10 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     c->d_acc.ensure((size_t)P.tot);
     const bool feats = p_learned > 0.f || record_max > 0;
     if (feats) c->d_x16.ensure((size_t)nch * mlp::IN);
-    if (p_learned > 0.f) c->mlp.ensure((int)nch);
+    if (p_learned > 0.f) {
+        c->mlp.ensure((int)nch);
+        c->mlp.prepare(c->stream);                  // nothing may allocate inside the capture
+    }
     MoveSet ms{nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr};
     if (record_max > 0) {
         c->d_mx.ensure((size_t)record_max * mlp::IN);

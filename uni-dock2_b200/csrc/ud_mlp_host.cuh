@@ -95,16 +95,21 @@ struct MlpState {
         }
     }
 
+    // one-time setup of the tcgen05 path (kernel attributes, error flag); also called before
+    // a CUDA graph capture of the forward pass, which must not allocate
+    void prepare(cudaStream_t s) {
+        if (!use_tc || tc_attr) return;
+        ck(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
+        ck(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
+        tc_err.ensure(1);
+        ck(cudaMemsetAsync(tc_err.p, 0, sizeof(int), s), "memset");
+        tc_attr = true;
+    }
+
     // out[n x 64] (FP32) from x16[n x 672]
     void forward(cudaStream_t s, int n, const __nv_bfloat16* x) {
         if (use_tc) {
-            if (!tc_attr) {
-                ck(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
-                ck(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
-                tc_err.ensure(1);
-                ck(cudaMemsetAsync(tc_err.p, 0, sizeof(int), s), "memset");
-                tc_attr = true;
-            }
+            prepare(s);
             tc_layer(s, n, x, mlp::IN, mlp::OFF_W1, mlp::OFF_B1, mlp::HID, 1, h16[0].p, nullptr);
             tc_layer(s, n, h16[0].p, mlp::HID, mlp::OFF_W2, mlp::OFF_B2, mlp::HID, 1, h16[1].p, nullptr);
             tc_layer(s, n, h16[1].p, mlp::HID, mlp::OFF_W3, mlp::OFF_B3, mlp::HID, 1, h16[2].p, nullptr);

@@ -19,7 +19,10 @@ engine (libudock_b200.so) instead of the reference's CUDA engine:
 
 Additional optional keyword arguments (not in the reference): ``scoring`` ("grid" or
 "direct" intermolecular term during search), ``grid_precision`` ("f32" or "f16"),
-``grid_spacing`` (A).
+``grid_spacing`` (A), ``proposal_params`` (parameters of a trained move-proposal network, a
+flat float32 array or the path of one saved with numpy; grid scoring only), ``p_learned``
+(share of learned moves when a network is given, default 0.25), ``poses_per_chain`` (1-4
+poses kept per chain before clustering) and ``autotune`` (time chain packings per batch).
 """
 from __future__ import annotations
 
@@ -78,7 +81,8 @@ class DockingPipeline:
                  seed: int = 12345, bias: str = "no", bias_k: float = 0.1, constraint_docking: bool = False,
                  use_tor_lib: bool = False, energy_decomp: bool = False, gpu_device_id: int = 0,
                  name_json: str = "from_python_obj", max_gpu_mem: int = 0,
-                 scoring: str = "grid", grid_precision: str = "f32", grid_spacing: float = 0.375):
+                 scoring: str = "grid", grid_precision: str = "f32", grid_spacing: float = 0.375,
+                 proposal_params=None, p_learned: float = 0.25, poses_per_chain: int = 1, autotune: bool = False):
         self.output_dir = output_dir
         self.box = Box.from_center_size([center_x, center_y, center_z], [size_x, size_y, size_z])
         self.task = task
@@ -103,6 +107,12 @@ class DockingPipeline:
         self.scoring = scoring
         self.grid_precision = grid_precision
         self.grid_spacing = float(grid_spacing)
+        if isinstance(proposal_params, str):
+            proposal_params = np.load(proposal_params)
+        self.proposal_params = None if proposal_params is None else np.asarray(proposal_params, np.float32)
+        self.p_learned = float(p_learned)
+        self.poses_per_chain = int(poses_per_chain)
+        self.autotune = bool(autotune)
         self._receptor: List = []
         self._ligands: Dict[str, dict] = {}
         self.last_stats: Dict[str, float] = {}
@@ -182,6 +192,10 @@ class DockingPipeline:
         try:
             eng.set_flags(self.constraint_docking, p["bias_type"], self.bias_k)
             eng.set_receptor(rec.xyz, rec.types)
+            if self.poses_per_chain != 1:
+                eng.set_retain(self.poses_per_chain)
+            if self.autotune:
+                eng.set_autotune(True)
             mode = MODE_GRID if self.scoring == "grid" else MODE_DIRECT
             if mode == MODE_GRID:
                 mt = sorted(set(int(t) for l in ligs for t in l.types if t != 0))
@@ -189,6 +203,10 @@ class DockingPipeline:
                     eng.build_grid(self.grid_spacing, mt, GRID_F16 if self.grid_precision == "f16" else GRID_F32)
                 else:
                     mode = MODE_DIRECT
+            learned = None
+            if self.proposal_params is not None and mode == MODE_GRID and p["mc_steps"] > 0:
+                eng.mlp_set_params(self.proposal_params)
+                learned = self.p_learned
             opt_steps = p["opt_steps"]
             batch_id = 0
             nevals = 0
@@ -203,7 +221,7 @@ class DockingPipeline:
                                    opt_steps=opt_steps, refine_steps=p["refine_steps"], num_pose=p["num_pose"],
                                    rmsd_limit=p["rmsd_limit"], energy_range=p["energy_range"],
                                    randomize=p["randomize"], mode=mode, final_mode=MODE_DIRECT,
-                                   energy_decomp=self.energy_decomp)
+                                   energy_decomp=self.energy_decomp, p_learned=learned)
                 nevals += ne
                 fp = os.path.join(self.output_dir, f"{self.name_json}_{batch_id}.json")
                 self._dump(fp, bl, res)
