@@ -114,4 +114,27 @@ void udref_score_batch(int npose, int natom, const Real* coords, const int* type
     }
 }
 
+// The reference's per-atom decomposition of the intermolecular energy
+// (score_decomp, score.cpp:114-147): out5[natom][5] = gauss1, gauss2, repulsion,
+// hydrophobic, hbond.
+void udref_score_decomp(int natom, const Real* coords, const int* types, int nrec, const Real* rec_xyz,
+                        const int* rec_types, Real* out5) {
+    UDFixMol fix;
+    fix.natom = nrec;
+    fix.coords.assign(rec_xyz, rec_xyz + 3 * nrec);
+    fix.vina_types.assign(rec_types, rec_types + nrec);
+    UDFlexMol m;
+    m.natom = natom;
+    m.vina_types.assign(types, types + natom);
+    std::vector<AtomEnergyDecomp> d;
+    score_decomp(d, coords, fix, m);
+    for (int i = 0; i < natom; i++) {
+        out5[5 * i + 0] = d[i].gauss1;
+        out5[5 * i + 1] = d[i].gauss2;
+        out5[5 * i + 2] = d[i].repulsion;
+        out5[5 * i + 3] = d[i].hydrophobic;
+        out5[5 * i + 4] = d[i].hbond;
+    }
+}
+
 }  // extern "C"

@@ -141,3 +141,35 @@ def test_fp16_maps_error_reported(gpu_sys):
     err = np.abs(e16 - e32) / np.maximum(1.0, np.abs(e32))
     print(f"FP16-vs-FP32 map energy error: max {err.max():.3e} mean {err.mean():.3e}")
     assert err.max() < 5e-3
+
+
+def test_energy_decomposition_matches_reference(gpu_sys, oracle64):
+    """Per-atom decomposition of the intermolecular energy (energy_decomp) against the
+    reference's own score_decomp (src/score/score.cpp:114-147, through oracle/_ref)."""
+    import os
+    import ctypes as C
+    from ud2b200 import MODE_DIRECT
+    ref = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libudref_f64.so")
+    if not os.path.exists(ref):
+        pytest.skip("the reference's score_decomp was not built")
+    R = C.CDLL(ref)
+    eng, box, rec = gpu_sys["eng"], gpu_sys["box"], gpu_sys["rec"]
+    env = oracle64.make_env(rec, box, mode="direct")
+    rng = np.random.default_rng(19)
+    pl, xs = [], []
+    for li, lig in enumerate(gpu_sys["ligs"]):
+        for p in perturbed_poses(oracle64, oracle64.ligand(lig), env, lig, rng, 4, box):
+            pl.append(li); xs.append(p["coords"])
+    _, dec = eng.score_terms(pl, xs, mode=MODE_DIRECT, decomp=True)
+    rx = rec.xyz.astype(np.float64).reshape(-1)
+    off = 0
+    for k, li in enumerate(pl):
+        lig = gpu_sys["ligs"][li]
+        want = np.zeros(5 * lig.natom)
+        x64 = xs[k].astype(np.float64).reshape(-1)
+        R.udref_score_decomp(C.c_int(lig.natom), x64.ctypes.data_as(C.c_void_p), lig.types.ctypes.data_as(C.c_void_p),
+                             C.c_int(rec.natom), rx.ctypes.data_as(C.c_void_p), rec.types.ctypes.data_as(C.c_void_p),
+                             want.ctypes.data_as(C.c_void_p))
+        got = dec[off:off + 5 * lig.natom]
+        off += 5 * lig.natom
+        assert np.all(np.abs(got - want) <= 1e-4 * np.maximum(1.0, np.abs(want))), (k, np.max(np.abs(got - want)))

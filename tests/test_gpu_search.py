@@ -228,3 +228,28 @@ def test_retained_poses_and_1024_pose_clustering(gpu_sys, oracle64):
         assert agree >= 0.95 * total
     finally:
         eng.set_retain(1)
+
+
+def test_constraint_docking_keeps_the_root_fragment(gpu_sys):
+    """Constraint docking (no translation or rotation, src/cuda/mc.cu:159-166,
+    bfgs.cuh:176,571): atoms that no torsion moves keep their input coordinates exactly in
+    every chain's pose, and the rigid-body gradient is zero."""
+    from ud2b200 import MODE_GRID
+    eng = gpu_sys["eng"]
+    eng.set_flags(True, 0, 0.1)
+    try:
+        eng.search(seed=8, nchain=16, mc_steps=6, opt_steps=5, randomize=True)
+        for li, lig in enumerate(gpu_sys["ligs"]):
+            moved = np.zeros(lig.natom, bool)
+            for r in lig.rotated:
+                moved[r] = True
+            root = np.where(~moved)[0]
+            recs = eng.chain_poses(li)
+            x = recs[:, 8:8 + 3 * lig.natom].reshape(len(recs), lig.natom, 3)
+            assert np.array_equal(x[:, root, :], np.broadcast_to(lig.coords[root], x[:, root, :].shape))
+        lig = gpu_sys["ligs"][-1]
+        _, gs = eng.score_batch([len(gpu_sys["ligs"]) - 1], [lig.coords], lig.center[None, :],
+                                np.zeros((1, 3), np.float32), mode=MODE_GRID, vcap=10.0)
+        assert np.all(gs[0][:6] == 0.0)
+    finally:
+        eng.set_flags(False, 0, 0.1)
