@@ -466,8 +466,9 @@ __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x
     int i1 = min(max((int)floorf(u1), 0), g.gy - 2);
     int i2 = min(max((int)floorf(u2), 0), g.gz - 2);
     const float fx = u0 - (float)i0, fy = u1 - (float)i1, fz = u2 - (float)i2;
-    const size_t sy = g.gx, sz = (size_t)g.gx * g.gy;
-    const size_t base = (size_t)map * ((size_t)g.gz * sz) + (size_t)i2 * sz + (size_t)i1 * sy + i0;
+    // 32-bit indices: the maps of one grid hold fewer than 2^31 values (20 x 81^3 at 30 A)
+    const int sy = g.gx, sz = g.gx * g.gy;
+    const int base = (map * g.gz + i2) * sz + i1 * sy + i0;
     float v0, v1, v2, v3, v4, v5, v6, v7;
     if (g.use_f16) {
         const __half* m = g.f16 + base;

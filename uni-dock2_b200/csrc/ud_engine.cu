@@ -1307,6 +1307,8 @@ int ud_build_grid(ud_ctx* c, float spacing, int nmaps, const int* map_types, int
         c->nmaps = nmaps;
         c->ligs_dirty = true;          // map slots of loaded ligands change
         long long npt = (long long)c->gdim[0] * c->gdim[1] * c->gdim[2];
+        if (npt * nmaps >= (1LL << 31))
+            throw Fail(UD_EINVAL, "grid too large: the maps must hold fewer than 2^31 values (larger spacing or box)");
         c->d_maps32.ensure((size_t)npt * nmaps);
         c->d_maps16.ensure((size_t)npt * nmaps);
         int threads = 256;
