@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--learned-steps", type=int, default=1000, help="MC steps of the learned-proposal engine")
     ap.add_argument("--p-learned", type=float, default=0.25, help="share of learned moves")
     ap.add_argument("--train-ligands", type=int, default=37, help="training ligands per seed (4 seeds)")
+    ap.add_argument("--train-epochs", type=int, default=6, help="epochs of network training")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -399,7 +400,7 @@ def run_ours(a):
         # proposal network trained on the GPU from the plain engine's own searches
         from ud2b200.learned import train_proposal
         params, trep = train_proposal(box, rec, tsets, mt, opt_steps=opt, nchain=w["chains"], mc_steps=150,
-                                      target=1, epochs=6, batch=1024, lr=1e-3, seed=1, device=local)
+                                      target=1, epochs=a.train_epochs, batch=1024, lr=1e-3, seed=1, device=local)
         eng.mlp_set_params(params)
         # the method without the network: the fused plain engine at the learned engine's steps
         res_eq, _ = eng.dock(**base_kw, mc_steps=a.learned_steps, fetch=True)
