@@ -9,6 +9,12 @@
 //                  work items in cost order from a global counter (src/cuda/mc.cu:109-448)
 //   k_cluster      CTA per ligand: energy ranking + greedy RMSD leaders (src/cuda/cluster.cu)
 //   k_filter       CTA per ligand: energy_range / num_pose filter (src/task/DockTask.cpp:188-220)
+//   k_gather       output records of the selected poses
+//   k_learn_step   one MC step of every chain per launch (the learned-proposal search; the
+//                  step function is k_search's), with k_learn_features (network input per
+//                  chain), k_step_advance, and k_lig_best / k_label_moves (move recording)
+//   k_pose_offsets prefix sums for ud_score_batch_noalloc
+// Network kernels (tcgen05 forward GEMM, mma.sync GEMM, loss, backward, Adam): ud_mlp.cuh.
 // Host orchestration replaces DockTask::run (src/task/DockTask.cpp:39-123).
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
