@@ -160,8 +160,69 @@ def test_pipeline_run_fails_loudly_without_gpu(tmp_path):
 
 
 def test_json_number_format():
+    """rapidjson's Double with 3 decimal places (include/rapidjson/internal/dtoa.h, Prettify):
+    truncation of the shortest digits, trailing zeros dropped keeping one, the sign kept on
+    values that truncate to zero; non-finite values and |v| > 1e6 clamped (json.cpp:78-85)."""
     from unidock_engine.api.python.pipeline import _fmt
-    assert _fmt(-7.23456) == "-7.234"
-    assert _fmt(12.0) == "12.0"
-    assert _fmt(float("nan")) == "1000000.0"
-    assert _fmt(3e7) == "1000000.0"
+    cases = [(-7.23456, "-7.234"), (12.0, "12.0"), (float("nan"), "1000000.0"), (3e7, "1000000.0"),
+             (-3e7, "-1000000.0"), (float("-inf"), "1000000.0"), (0.1, "0.1"), (12.3004, "12.3"),
+             (1.102, "1.101"), (1.25, "1.25"), (-0.0004, "-0.0"), (1e-7, "0.0"), (0.0, "0.0"), (-0.0, "-0.0"),
+             (0.30000001, "0.3"), (999999.9, "999999.875"), (0.001, "0.001")]
+    for v, want in cases:
+        assert _fmt(v) == want, (v, _fmt(v), want)
+
+
+def test_json_number_format_vectorised_matches_scalar():
+    from unidock_engine.api.python.pipeline import _fmt, _fmt_array
+    rng = np.random.default_rng(4)
+    parts = [rng.normal(0, s, 20000) for s in (1e-3, 0.1, 1.0, 30.0, 1e3, 1e5, 3e6)]
+    parts.append(np.round(rng.normal(0, 10, 20000), 3))             # values near multiples of 1/1000
+    parts.append(rng.integers(-2000, 2000, 5000) / 8.0)             # exact multiples
+    parts.append(np.array([0.0, -0.0, np.nan, np.inf, -np.inf, 1e-40, -1e-40, 1e6, -1e6]))
+    v = np.concatenate(parts).astype(np.float32)
+    got = _fmt_array(v)
+    want = [_fmt(float(x)) for x in v]
+    bad = [(float(x), a, b) for x, a, b in zip(v, got, want) if a != b]
+    assert not bad, bad[:10]
+
+
+def test_json_writer_layout(tmp_path, small_system):
+    """The batch file: per ligand its poses with the 7-value energy vector (affinity from the
+    rank-1 intra, float32 arithmetic), 3N coordinates, T dihedrals in degrees and the
+    per-atom decomposition, each value printed by the scalar rule."""
+    import json
+    from ud2b200.engine import DockResult, record_len
+    from ud2b200.model import RAD2DEG_F
+    from unidock_engine.api.python.pipeline import DockingPipeline, W_CONF, _fmt
+    rng = np.random.default_rng(5)
+    ligs = small_system["ligs"]
+    res = []
+    for i, lig in enumerate(ligs):
+        k = i % 3                                                       # 0 poses for the first ligand
+        recs = [rng.normal(0, 5, record_len(lig)).astype(np.float32) for _ in range(k)]
+        res.append(DockResult(recs, rng.normal(0, 3, (k, 4)).astype(np.float32),
+                              rng.normal(0, 1, (k, lig.natom, 5)).astype(np.float32)))
+    c = small_system["center"]
+    p = DockingPipeline(output_dir=str(tmp_path), center_x=c[0], center_y=c[1], center_z=c[2], size_x=20,
+                        size_y=20, size_z=20, energy_decomp=True)
+    fp = str(tmp_path / "b.json")
+    p._dump(fp, ligs, res)
+    text = open(fp).read()
+    got = json.loads(text)
+    assert list(got) == [l.name for l in ligs]
+    F = np.float32
+    for lig, r in zip(ligs, res):
+        poses = got[lig.name]
+        assert len(poses) == len(r.records)
+        for j, (rec, pose) in enumerate(zip(r.records, poses)):
+            intra, inter, pen, bias = (F(x) for x in r.terms[j])
+            total = F(F(intra + inter) + pen)
+            e_inter = F(total - F(r.terms[0, 0]))
+            aff = F(e_inter / F(F(1) + W_CONF * F(lig.ntors)))
+            want = [aff, total, intra, inter, pen, F(aff - e_inter), bias]
+            n3 = 3 * lig.natom
+            exp = ('{"energy":[' + ",".join(_fmt(x) for x in want) + '],"coords":[' +
+                   ",".join(_fmt(x) for x in rec[8:8 + n3]) + '],"dihedrals":[' +
+                   ",".join(_fmt(F(x * RAD2DEG_F)) for x in rec[8 + n3:8 + n3 + lig.ntors]) +
+                   '],"decomp":[' + ",".join("[" + ",".join(_fmt(x) for x in a) + "]" for a in r.decomp[j]) + "]}")
+            assert exp in text, (lig.name, j)

@@ -31,12 +31,13 @@ import logging
 import math
 import os
 import time
+from decimal import ROUND_DOWN, Decimal
 from typing import Dict, List, Optional
 
 import numpy as np
 
 from ud2b200.batching import batches
-from ud2b200.engine import Engine, EngineError, MODE_DIRECT, MODE_GRID, GRID_F16, GRID_F32, split_record
+from ud2b200.engine import Engine, EngineError, MODE_DIRECT, MODE_GRID, GRID_F16, GRID_F32
 from ud2b200.model import Box, F32, RAD2DEG_F, parse_ligands, parse_receptor
 
 log = logging.getLogger("unidock_engine")
@@ -53,22 +54,33 @@ def _safe(v: float) -> float:
 
 
 def _fmt(v: float) -> str:
-    """Shortest float text truncated to 3 decimals (rapidjson SetMaxDecimalPlaces(3))."""
+    """One value as the reference's writer prints it: the float widened to double, its
+    shortest round-trip digits truncated to 3 decimals, trailing zeros dropped keeping one
+    (rapidjson Writer::Double with SetMaxDecimalPlaces(3): include/rapidjson/internal/dtoa.h,
+    Prettify).  The scalar statement of the rule; ``_fmt_array`` is the fast one."""
     v = _safe(float(np.float32(v)))
-    s = repr(float(np.float32(v)))
-    if "e" in s or "E" in s:
-        s = f"{v:.6f}"
-    if "." in s:
-        ip, fp = s.split(".", 1)
-        fp = fp[:3]
-        s = ip + "." + (fp if fp else "0")
-    else:
-        s = s + ".0"
-    return s
+    q = int(Decimal(repr(abs(v))).scaleb(3).to_integral_value(rounding=ROUND_DOWN))
+    ip, fr = divmod(q, 1000)
+    return ("-" if math.copysign(1.0, v) < 0 else "") + str(ip) + _FRAC[fr]
 
 
-def _json_list(vals) -> str:
-    return "[" + ",".join(_fmt(x) for x in vals) + "]"
+# ".d", ".dd" or ".ddd" for 0..999 thousandths, trailing zeros dropped keeping one digit
+_FRAC = ["." + (("%03d" % i).rstrip("0") or "0") for i in range(1000)]
+_FRAC_NP = np.array(_FRAC)
+
+
+def _fmt_array(vals) -> List[str]:
+    """``_fmt`` of every value, vectorised.  A float32 value times 1000 is exact in double
+    (24 + 10 significant bits), so flooring it gives the truncated thousandths of the exact
+    value; those equal the truncation of the shortest digits, because a float32 value that
+    is not a multiple of 1/1000 lies further from one (about 2^-34 of its magnitude at
+    least: its ulp over 1000) than its shortest double digits lie from it (2^-53)."""
+    v = np.asarray(vals, np.float32).astype(np.float64).reshape(-1)
+    v = np.where(np.isfinite(v), np.clip(v, -MAX_SAFE, MAX_SAFE), MAX_SAFE)
+    q = np.floor(np.abs(v) * 1000.0).astype(np.int64)
+    s = np.strings.add(np.strings.add(np.where(np.signbit(v), "-", ""), (q // 1000).astype(str)),
+                       _FRAC_NP[q % 1000])
+    return s.tolist()
 
 
 class DockingPipeline:
@@ -233,21 +245,33 @@ class DockingPipeline:
     def _dump(self, fp: str, ligs, results) -> None:
         parts = []
         for lig, r in zip(ligs, results):
+            n3, nt = 3 * lig.natom, lig.ntors
+            k = len(r.records)
+            if k == 0:
+                parts.append(json.dumps(lig.name) + ":[]")
+                continue
+            # the energy vector in float32 arithmetic (DockTask.cpp:224-282)
+            intra, inter, pen, bias = (r.terms[:k, c].astype(np.float32) for c in range(4))
+            total = (intra + inter) + pen
+            e_inter = total - intra[0]
+            aff = e_inter / (F32(1) + W_CONF * F32(nt))
+            conf = aff - e_inter
+            recs = np.stack(r.records)
+            vals = [np.stack([aff, total, intra, inter, pen, conf, bias], axis=1), recs[:, 8:8 + n3],
+                    recs[:, 8 + n3:8 + n3 + nt] * RAD2DEG_F]
+            dec = self.energy_decomp and r.decomp is not None
+            if dec:
+                vals.append(r.decomp[:k].reshape(k, -1))
+            txt = _fmt_array(np.concatenate([v.astype(np.float32) for v in vals], axis=1))
+            w = len(txt) // k
             poses = []
-            intra_r1 = F32(r.terms[0, 0]) if len(r.records) else F32(0)
-            for k, rec in enumerate(r.records):
-                pose = split_record(lig, rec)
-                intra, inter, pen, bias = (F32(v) for v in r.terms[k])
-                total = F32(F32(intra + inter) + pen)
-                e_inter = F32(total - intra_r1)
-                aff = F32(e_inter / F32(F32(1) + W_CONF * F32(lig.ntors)))
-                conf = F32(aff - e_inter)
-                energy = [aff, total, intra, inter, pen, conf, bias]
-                dih = [F32(d * RAD2DEG_F) for d in pose["dihedrals"]]
-                s = '{"energy":' + _json_list(energy) + ',"coords":' + _json_list(pose["coords"].reshape(-1)) + \
-                    ',"dihedrals":' + _json_list(dih)
-                if self.energy_decomp and r.decomp is not None:
-                    s += ',"decomp":[' + ",".join(_json_list(a) for a in r.decomp[k]) + "]"
+            for j in range(k):
+                t = txt[j * w:(j + 1) * w]
+                s = '{"energy":[' + ",".join(t[:7]) + '],"coords":[' + ",".join(t[7:7 + n3]) + \
+                    '],"dihedrals":[' + ",".join(t[7 + n3:7 + n3 + nt]) + "]"
+                if dec:
+                    d = t[7 + n3 + nt:]
+                    s += ',"decomp":[' + ",".join("[" + ",".join(d[a:a + 5]) + "]" for a in range(0, len(d), 5)) + "]"
                 poses.append(s + "}")
             parts.append(json.dumps(lig.name) + ":[" + ",".join(poses) + "]")
         text = "{" + ",".join(parts) + "}"
