@@ -24,6 +24,7 @@ synchronisation and its time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import glob
 import json
 import math
 import os
@@ -325,6 +326,10 @@ def run_reference_gpu(a):
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=3600)
         line = [l for l in r.stdout.splitlines() if l.startswith("{")]
         ref = json.loads(line[-1]) if line else {"rc": r.returncode}
+        ref_poses = {}
+        for fp in sorted(glob.glob(os.path.join(tmp, "out", "udref_*.json"))):
+            with open(fp) as f:
+                ref_poses.update(json.load(f))
     rec = parse_receptor(rows, box)
     eng = Engine(box)
     eng.set_receptor(rec.xyz, rec.types)
@@ -337,6 +342,14 @@ def run_reference_gpu(a):
     ours_s = time.perf_counter() - t0
     eng.close()
     full = w["mc_steps"] / steps
+    # best scores: total (intra + inter + penalty) of each ligand's top-ranked pose; the
+    # reference's from its JSON files (energy[1]), 3 decimals
+    quality = None
+    if all(n in ref_poses and ref_poses[n] for n in ligd):
+        ref_top = np.array([ref_poses[n][0]["energy"][1] for n in ligd], np.float64)
+        gap = np.array(top_scores(res), np.float64) - ref_top
+        quality = {"within_0.3_of_reference": float(np.mean(gap <= 0.3)), "mean_gap": float(gap.mean()),
+                   "max_gap": float(gap.max()), "better_than_reference": float(np.mean(gap < -1e-3))}
     out = {"impl": "reference-gpu", "metric": METRIC, "unit": UNIT, "workload": a.workload, "ligands": len(ligs),
            "chains": w["chains"], "mc_steps_run": steps, "mc_steps_workload": w["mc_steps"], "opt_steps": opt,
            "reference": {"rc": ref.get("rc"), "seconds": ref.get("seconds"),
@@ -344,6 +357,7 @@ def run_reference_gpu(a):
                          "engine": "the reference's core_pipeline (direct pair sums), built from its sources"},
            "ours": {"seconds": ours_s, "value": len(ligs) / (ours_s * full),
                     "engine": "this engine, ud_dock with grid maps (grid build included)"},
+           "quality": quality,
            "note": "wall times of one call each on the same GPU and inputs; ligands/s extrapolated linearly "
                    f"from {steps} to {w['mc_steps']} MC steps"}
     print(json.dumps(out), flush=True)

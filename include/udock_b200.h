@@ -182,6 +182,8 @@ typedef struct {
     int mode;            /* UD_MODE_GRID or UD_MODE_DIRECT for the search */
     int final_mode;      /* scoring of output poses: UD_MODE_DIRECT (reference) or grid */
     int energy_decomp;
+    int refine_mode;     /* scoring of the refinement BFGS: UD_MODE_DIRECT (exact pair sums, as
+                            the reference's optimize_cu, src/cuda/optimize.cu:14-77) or grid */
 } ud_dock_params;
 
 int ud_dock(ud_ctx* ctx, const ud_dock_params* params, long long* out_nevals);

@@ -1,0 +1,114 @@
+"""The reference's own CUDA engine (Uni-Dock2's core_pipeline, compiled from its sources into
+oracle/_ref/udref_dock) and this engine on the same inputs and settings, on the same GPU.
+
+* every pose the reference engine writes (its JSON files, src/format/json.cpp:88-191) is
+  scored here with the final-score path (ud_score_terms, direct sums): intra, inter and
+  penalty equal the reference's energy vector within the error of its 3-decimal coordinates,
+  and the affinity follows from total and the rank-1 intra as the reference computes it
+  (src/task/DockTask.cpp:224-282, vina_conf_indep in src/score/vina.h:202-204);
+* best scores of the two searches (different RNG streams, grid maps here, direct sums in the
+  reference) agree as distributions: the mean gap of the top-pose totals is printed and
+  bounded.
+
+Skipped when oracle/_ref/udref_dock has not been built (it needs the reference sources)."""
+import glob
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "oracle", "_ref", "udref_dock")
+W_CONF = 0.05846
+
+SETTINGS = dict(nchain=128, mc_steps=60, refine_steps=2, num_pose=4, rmsd_limit=1.0, energy_range=10.0, seed=5)
+
+
+@pytest.fixture(scope="module")
+def ref_run(small_system, tmp_path_factory):
+    if not os.path.exists(EXE):
+        pytest.skip("oracle/_ref/udref_dock not built")
+    from ud2b200.batching import heuristic_opt_steps
+    ligs = small_system["ligs"]
+    opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
+    tmp = tmp_path_factory.mktemp("udref")
+    inp = tmp / "input.json"
+    inp.write_text(json.dumps(dict(receptor=small_system["rows"], **small_system["ligd"])))
+    out = tmp / "out"
+    out.mkdir()
+    c = [float(v) for v in small_system["center"]]
+    s = SETTINGS
+    cmd = [EXE, str(inp), str(out), *map(str, c), "20.0", "20.0", "20.0", str(s["nchain"]), str(s["mc_steps"]),
+           str(opt), str(s["refine_steps"]), str(s["num_pose"]), str(s["rmsd_limit"]), str(s["energy_range"]),
+           str(s["seed"]), "0"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    poses = {}
+    for fp in sorted(glob.glob(str(out / "udref_*.json"))):
+        poses.update(json.load(open(fp)))
+    assert set(poses) == set(small_system["ligd"])
+    return dict(poses=poses, opt=opt)
+
+
+def test_reference_engine_poses_rescored_here(small_system, ref_run):
+    from ud2b200 import Engine, MODE_DIRECT
+    ligs = small_system["ligs"]
+    names = list(small_system["ligd"])
+    eng = Engine(small_system["box"])
+    try:
+        rows = np.asarray([r[:4] for r in small_system["rows"]], np.float64)
+        eng.set_receptor(rows[:, :3].astype(np.float32), rows[:, 3].astype(np.int32))
+        eng.add_ligands(ligs)
+        pl, xs, want = [], [], []
+        for li, name in enumerate(names):
+            lig = ligs[li]
+            poses = ref_run["poses"][name]
+            assert 1 <= len(poses) <= SETTINGS["num_pose"]
+            intra_r1 = poses[0]["energy"][2]
+            for p in poses:
+                e = p["energy"]
+                assert len(p["coords"]) == 3 * lig.natom and len(p["dihedrals"]) == lig.ntors
+                # affinity from total and the rank-1 intra (3-decimal rounding of each value)
+                aff = (e[1] - intra_r1) / (1.0 + W_CONF * lig.ntors)
+                assert abs(aff - e[0]) <= 2e-3, (name, e)
+                assert abs(e[1] - (e[2] + e[3] + e[4])) <= 2e-3, (name, e)
+                pl.append(li)
+                xs.append(np.asarray(p["coords"], np.float32).reshape(lig.natom, 3))
+                want.append(e)
+        terms, _ = eng.score_terms(pl, xs, mode=MODE_DIRECT)
+        want = np.asarray(want, np.float64)
+        got = terms.astype(np.float64)
+        # columns: intra, inter, penalty (the reference: energy[2], [3], [4])
+        err = np.abs(got[:, :3] - want[:, 2:5])
+        print(f"{len(pl)} reference poses rescored: max |d| intra {err[:, 0].max():.2e}, "
+              f"inter {err[:, 1].max():.2e}, penalty {err[:, 2].max():.2e} kcal/mol")
+        tol = 0.02 + 2e-3 * np.abs(want[:, 2:5])
+        assert np.all(err <= tol), (err.max(axis=0), np.argmax(err, axis=0))
+    finally:
+        eng.close()
+
+
+def test_best_scores_agree_with_reference_engine(small_system, ref_run):
+    from gpu_helpers import engine_for
+    names = list(small_system["ligd"])
+    eng, _ = engine_for(small_system)
+    try:
+        s = SETTINGS
+        res, _ = eng.dock(seed=s["seed"], nchain=s["nchain"], mc_steps=s["mc_steps"], opt_steps=ref_run["opt"],
+                          refine_steps=s["refine_steps"], num_pose=s["num_pose"], rmsd_limit=s["rmsd_limit"],
+                          energy_range=s["energy_range"])
+    finally:
+        eng.close()
+    ours = np.array([float(r.terms[0, :3].sum()) for r in res])
+    ref = np.array([ref_run["poses"][n][0]["energy"][1] for n in names])
+    gap = ours - ref
+    print("top-pose totals, this engine:", np.round(ours, 3).tolist())
+    print("top-pose totals, reference engine:", np.round(ref, 3).tolist())
+    print(f"gap (this - reference): mean {gap.mean():+.3f}, max {gap.max():+.3f} kcal/mol")
+    assert np.all(np.isfinite(ours))
+    assert gap.mean() <= 0.5
+    assert np.all(gap <= 2.0)

@@ -2041,7 +2041,7 @@ int ud_cluster(ud_ctx* c, float rmsd_limit, int* out_leaders, int* out_counts) {
 static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long long* out_nevals) {
     try {
         if (!c || !p || p->nchain <= 0 || p->mc_steps < 0 || p->opt_steps < 0 || p->num_pose <= 0 ||
-            p->refine_steps < 0)
+            p->refine_steps < 0 || (p->refine_mode != UD_MODE_DIRECT && p->refine_mode != UD_MODE_GRID))
             throw Fail(UD_EINVAL, "invalid dock parameters");
         ck(cudaSetDevice(c->device), "cudaSetDevice");
         int nlig = (int)c->h_ligs.size();
@@ -2057,9 +2057,9 @@ static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long l
         launch_cluster(c, p->rmsd_limit);
         c->counters[2]++;
         c->rec(2);
-        Env env = make_env(c, p->mode);
-        // refinement of every cluster leader: the (ligand, chain) list is built on the host
-        // from the leader counts
+        // refinement of every cluster leader (on exact pair sums unless refine_mode says
+        // grid): the (ligand, chain) list is built on the host from the leader counts
+        Env env = make_env(c, p->refine_mode);
         std::vector<int> counts(nlig);
         ck(cudaMemcpyAsync(counts.data(), c->d_counts.p, nlig * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "D2H");
         const int nrec_lig = c->nchain;                 // records per ligand (chains x retained)

@@ -104,7 +104,7 @@ class DockParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("nchain", C.c_int), ("mc_steps", C.c_int), ("opt_steps", C.c_int),
                 ("refine_steps", C.c_int), ("num_pose", C.c_int), ("rmsd_limit", C.c_float),
                 ("energy_range", C.c_float), ("randomize", C.c_int), ("mode", C.c_int), ("final_mode", C.c_int),
-                ("energy_decomp", C.c_int)]
+                ("energy_decomp", C.c_int), ("refine_mode", C.c_int)]
 
 
 def _p(a: Optional[np.ndarray]):
@@ -423,11 +423,13 @@ class Engine:
     def dock(self, seed: int, nchain: int, mc_steps: int, opt_steps: int, refine_steps: int, num_pose: int,
              rmsd_limit: float, energy_range: float, randomize: bool = True, mode: int = MODE_GRID,
              final_mode: int = MODE_DIRECT, energy_decomp: bool = False,
-             fetch: bool = True, p_learned: Optional[float] = None) -> Tuple[Optional[List[DockResult]], int]:
+             fetch: bool = True, p_learned: Optional[float] = None,
+             refine_mode: int = MODE_DIRECT) -> Tuple[Optional[List[DockResult]], int]:
         """Dock the loaded ligands (search, clustering, refinement, filter, final scores);
-        p_learned: None for the fused plain search, else the learned-proposal search."""
+        p_learned: None for the fused plain search, else the learned-proposal search;
+        refine_mode: scoring of the refinement (exact pair sums by default, as the reference)."""
         p = DockParams(seed & (2 ** 64 - 1), nchain, mc_steps, opt_steps, refine_steps, num_pose, rmsd_limit,
-                       energy_range, int(randomize), mode, final_mode, int(energy_decomp))
+                       energy_range, int(randomize), mode, final_mode, int(energy_decomp), int(refine_mode))
         ne = C.c_longlong(0)
         if p_learned is None:
             self._check(self.L.ud_dock(self.h, C.byref(p), C.byref(ne)))
