@@ -128,6 +128,21 @@ def test_learned_search_p0_matches_fused_search(search_sys):
         assert np.array_equal(got, want[l], equal_nan=True), l
 
 
+def test_learned_search_p0_matches_fused_search_wide_ctas(search_sys):
+    """The same with 12-warp CTAs (the 384-thread instantiations of both kernels)."""
+    eng = search_sys["eng"]
+    eng.set_packing(12, 1)
+    try:
+        eng.search(seed=22, nchain=24, mc_steps=6, opt_steps=5, randomize=True)
+        want = [eng.chain_poses(l).copy() for l in range(len(search_sys["ligs"]))]
+        eng.search_learned(seed=22, nchain=24, mc_steps=6, opt_steps=5, p_learned=0.0)
+        assert eng.search_shape()["warps_per_cta"] == 12
+        for l in range(len(search_sys["ligs"])):
+            assert np.array_equal(eng.chain_poses(l), want[l], equal_nan=True), l
+    finally:
+        eng.set_packing(0, 0)
+
+
 def test_collect_moves_and_learned_search(search_sys):
     eng = search_sys["eng"]
     ligs = search_sys["ligs"]

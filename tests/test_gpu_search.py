@@ -192,6 +192,28 @@ def test_autotuned_packing_gives_the_same_chains(gpu_sys):
         assert np.array_equal(x, y, equal_nan=True)
 
 
+def test_packings_give_the_same_chains(gpu_sys):
+    """Every chain packing (4, 8 or 12 warps per CTA; 1 or 2 chains per warp per work item)
+    runs the same chains: bit-identical records.  The 12-warp CTAs use the 384-thread
+    instantiation, the others the 256-thread ones."""
+    eng = gpu_sys["eng"]
+    nl = len(gpu_sys["ligs"])
+    eng.search(seed=7, nchain=40, mc_steps=8, opt_steps=6, randomize=True)
+    want = [eng.chain_poses(l).copy() for l in range(nl)]
+    print("default shape:", eng.search_shape())
+    try:
+        for w, k in [(12, 1), (12, 2), (8, 1), (8, 2), (4, 1), (4, 2)]:
+            eng.set_packing(w, k)
+            eng.search(seed=7, nchain=40, mc_steps=8, opt_steps=6, randomize=True)
+            sh = eng.search_shape()
+            assert sh["warps_per_cta"] == w and sh["chains_per_warp"] == k and sh["ctas_per_sm"] >= 1, sh
+            assert sh["register_class"] == (2 if w == 12 else sh["register_class"])
+            for l in range(nl):
+                assert np.array_equal(eng.chain_poses(l), want[l], equal_nan=True), (w, k, l)
+    finally:
+        eng.set_packing(0, 0)
+
+
 def test_retained_poses_and_1024_pose_clustering(gpu_sys, oracle64):
     """256 chains keeping 4 poses each.  A chain's kept energies are distinct successive
     bests (unused records: 1e9); the lowest agrees with the one-pose search's best for

@@ -523,10 +523,12 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
 // items from a global counter, re-stage the topology blob only when the ligand changes,
 // and their warps take the item's chains from a shared counter.  Large ligands are so
 // spread over many CTAs and the launch ends with the cheapest items.
-// MINB: 256-thread CTAs per SM the register budget is sized for (4: 64 registers, 3: 80);
-// the host picks the instantiation whose CTA count the shared memory allows.
-template <int MINB, int RMAX>
-__global__ void __launch_bounds__(256, MINB) k_search(const int* __restrict__ blobs,
+// NT, MINB: the largest CTA and the CTAs per SM the register budget is sized for (256
+// threads: 4 CTAs = 64 registers, 3 = 80; 384 threads: 2 CTAs = 80 registers); the host
+// picks the width and instantiation that keep the most warps resident (shared memory
+// holds one topology blob per CTA, so wide CTAs pay when the blob is large).
+template <int MINB, int RMAX, int NT = 256>
+__global__ void __launch_bounds__(NT, MINB) k_search(const int* __restrict__ blobs,
                                                 const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                 int nitems, Env env, SearchP sp, float* best, int* work_counter,
                                                 unsigned long long* nevals) {
@@ -832,8 +834,8 @@ __global__ void k_label_moves(const int* __restrict__ blobs, const LigDev* __res
     }
 }
 
-template <int MINB, int RMAX>
-__global__ void __launch_bounds__(256, MINB) k_learn_step(const int* __restrict__ blobs,
+template <int MINB, int RMAX, int NT = 256>
+__global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__ blobs,
                                                         const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                         int nitems, Env env, LearnP sp, const int* __restrict__ step_p,
                                                         float* acc, float* best, const float* __restrict__ prop_out,
@@ -1125,6 +1127,8 @@ struct ud_ctx {
     int moves_max = 0, moves_n = 0;
     // chain packing autotuner (warps per CTA, chains per warp per work item)
     int autotune = 0, tune_w = 8, tune_k = 0;
+    int pack_w = 0, pack_k = 0;               // ud_set_packing (0: chosen per batch)
+    int shape[4] = {0, 0, 0, 0};              // last search: W, CTAs per SM, minb, k
     int retain = 1;                                   // poses kept per chain
     long long tune_key = -1;
     // measurement
@@ -1746,14 +1750,14 @@ int ud_bfgs_batch(ud_ctx* c, int n, const int* pose_lig, float* records, int max
 // count) in descending ligand cost, uploaded with the work counter cleared.
 struct SearchPlan {
     int W = 0, grid = 0, nitems = 0, wsm = 0, blob_max = 0;
-    bool four = false;
+    int minb = 3;          // instantiation: 3 or 4 (256-thread bound), 2 (384-thread bound)
     size_t smem = 0;
     long long tot = 0;
 };
 
 extern "C++" {
 template <typename K>
-static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, int want_w = 8, int force_k = 0) {
+static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, K k12, int want_w = 0, int force_k = 0) {
     SearchPlan P;
     const int nlig = (int)c->h_ligs.size();
     std::vector<int> order(nlig);
@@ -1770,16 +1774,35 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, int want_w = 8,
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     P.blob_max = r4(c->max_stage);
-    P.W = pick_warps(c, P.wsm, P.blob_max, want_w);
-    P.smem = ((size_t)P.blob_max + (size_t)P.W * P.wsm) * 4;
     int smem_sm = 0;
     ck(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->device), "attribute");
-    // CTAs per SM the shared memory allows (1 KB per CTA is reserved by the runtime)
-    P.four = (size_t)smem_sm / (P.smem + 1024) >= 4;
-    K kern = P.four ? k4 : k3;
-    set_smem(kern, P.smem);
+    const long long lim = smem_limit(c) / 4 - 64;       // floats of one CTA's shared memory
+    // CTA widths 8, 12 and 4 warps (want_w > 0: that one only): per width the instantiation
+    // its shared memory allows (64 registers only where that reaches 32 warps per SM; 1 KB
+    // per CTA is reserved by the runtime), kept if it holds the most warps resident
     int per_sm = 0;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * P.W, P.smem), "occupancy");
+    K chosen = k3;
+    for (int w : {8, 12, 4}) {
+        if (want_w > 0 && w != want_w) continue;
+        if ((long long)P.blob_max + (long long)w * P.wsm > lim) continue;
+        const size_t smem = ((size_t)P.blob_max + (size_t)w * P.wsm) * 4;
+        const int by_smem = (int)((size_t)smem_sm / (smem + 1024));
+        const int minb = w == 12 ? 2 : (by_smem * w >= 32 ? 4 : 3);
+        K kern = minb == 2 ? k12 : (minb == 4 ? k4 : k3);
+        set_smem(kern, smem);
+        int n = 0;
+        ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, 32 * w, smem), "occupancy");
+        if (n * w > per_sm * P.W) { P.W = w; P.minb = minb; P.smem = smem; per_sm = n; chosen = kern; }
+    }
+    if (P.W == 0) {                                    // a ligand too large for 4 warps per CTA
+        P.W = pick_warps(c, P.wsm, P.blob_max, 4);
+        P.minb = 3;
+        P.smem = ((size_t)P.blob_max + (size_t)P.W * P.wsm) * 4;
+        chosen = k3;
+        set_smem(k3, P.smem);
+        ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k3, 32 * P.W, P.smem), "occupancy");
+    }
+    set_smem(chosen, P.smem);      // the candidates may have set a smaller size on the same kernel
     if (per_sm < 1) per_sm = 1;
     const long long resident = (long long)c->nsm * per_sm;
     // k chains per warp per item (W*k chains): the warps of a CTA share an item's chains
@@ -1797,6 +1820,7 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, int want_w = 8,
     c->d_items.upload(items.data(), items.size(), c->stream);
     P.nitems = (int)items.size();
     P.grid = (int)std::min((long long)P.nitems, resident);
+    c->shape[0] = P.W; c->shape[1] = per_sm; c->shape[2] = P.minb; c->shape[3] = k;
     c->d_counter.ensure(1);
     c->d_nevals.ensure(2);
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
@@ -1805,6 +1829,18 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, int want_w = 8,
     return P;
 }
 }  // extern "C++"
+
+using SearchKernel = void (*)(const int*, const LigDev*, const int4*, int, Env, SearchP, float*, int*,
+                              unsigned long long*);
+// the k_search instantiation of a plan (minb 3, 4: 256-thread bound; 2: 384-thread bound)
+static SearchKernel search_kernel(int minb, int rmax) {
+    if (rmax > 1) return minb == 4 ? k_search<4, 4> : (minb == 2 ? k_search<2, 4, 384> : k_search<3, 4>);
+    return minb == 4 ? k_search<4, 1> : (minb == 2 ? k_search<2, 1, 384> : k_search<3, 1>);
+}
+static SearchPlan plan_fused(ud_ctx* c, int nchain, int want_w = 0, int force_k = 0) {
+    const int r = c->retain;
+    return plan_search(c, nchain, search_kernel(3, r), search_kernel(4, r), search_kernel(2, r), want_w, force_k);
+}
 
 static void run_search_plan(ud_ctx* c, const SearchPlan& P, const Env& env, uint64_t seed, int nchain, int mc_steps,
                             int opt_steps, int randomize) {
@@ -1819,7 +1855,7 @@ static void run_search_plan(ud_ctx* c, const SearchPlan& P, const Env& env, uint
     sp.ws_max = P.wsm;
     sp.blob_max = P.blob_max;
     if (P.grid > 0) {
-        auto kern = c->retain > 1 ? (P.four ? k_search<4, 4> : k_search<3, 4>) : (P.four ? k_search<4, 1> : k_search<3, 1>);
+        const SearchKernel kern = search_kernel(P.minb, c->retain);
         kern<<<P.grid, 32 * P.W, P.smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, c->d_items.p, P.nitems, env, sp,
                                                       c->d_best.p, c->d_counter.p, c->d_nevals.p);
         ck(cudaGetLastError(), "k_search launch");
@@ -1827,7 +1863,7 @@ static void run_search_plan(ud_ctx* c, const SearchPlan& P, const Env& env, uint
     }
 }
 
-// Chain packing autotuner: warps per CTA (4 or 8) and chains per warp per work item
+// Chain packing autotuner: warps per CTA (8, 12 or 4) and chains per warp per work item
 // (1, 2 or 4), each timed with CUDA events on a short search of the batch itself
 // (3 MC steps); the fastest is kept for batches of the same shape.  A chain's result does
 // not depend on the packing (its random stream is indexed by chain, ligand and step).
@@ -1840,9 +1876,9 @@ static void autotune_search(ud_ctx* c, const Env& env, uint64_t seed, int nchain
     ck(cudaEventCreate(&e1), "event");
     float best_ms = 1e30f;
     int best_w = 8, best_k = 0;
-    for (int w : {8, 4})
+    for (int w : {8, 12, 4})
         for (int k : {1, 2, 4}) {
-            const SearchPlan P = plan_search(c, nchain, k_search<3, 1>, k_search<4, 1>, w, k);
+            const SearchPlan P = plan_fused(c, nchain, w, k);
             c->d_best.ensure((size_t)P.tot);
             ck(cudaEventRecord(e0, c->stream), "event");
             run_search_plan(c, P, env, seed, nchain, 3, opt_steps, randomize);
@@ -1863,12 +1899,10 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
     sync_ligs(c);
     Env env = make_env(c, mode);
     c->nchain = nchain * c->retain;                  // records per ligand
-    if (c->autotune) autotune_search(c, env, seed, nchain, opt_steps, randomize);
-    const SearchPlan P = c->retain > 1
-                             ? (c->autotune ? plan_search(c, nchain, k_search<3, 4>, k_search<4, 4>, c->tune_w, c->tune_k)
-                                            : plan_search(c, nchain, k_search<3, 4>, k_search<4, 4>))
-                             : (c->autotune ? plan_search(c, nchain, k_search<3, 1>, k_search<4, 1>, c->tune_w, c->tune_k)
-                                            : plan_search(c, nchain, k_search<3, 1>, k_search<4, 1>));
+    if (c->autotune && !(c->pack_w || c->pack_k)) autotune_search(c, env, seed, nchain, opt_steps, randomize);
+    const SearchPlan P = (c->pack_w || c->pack_k) ? plan_fused(c, nchain, c->pack_w, c->pack_k)
+                         : c->autotune         ? plan_fused(c, nchain, c->tune_w, c->tune_k)
+                                               : plan_fused(c, nchain);
     c->best_floats = P.tot;
     c->d_best.ensure((size_t)P.tot);
     run_search_plan(c, P, env, seed, nchain, mc_steps, opt_steps, randomize);
@@ -1891,8 +1925,11 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     for (const LigHost& h : c->h_ligs)
         if (h.natom > mlp::NATOM || h.ntors > mlp::TMAX)
             throw Fail(UD_EINVAL, "the proposal network covers ligands of at most 80 atoms and 20 torsions");
-    const SearchPlan P = c->retain > 1 ? plan_search(c, nchain, k_learn_step<3, 4>, k_learn_step<4, 4>)
-                                       : plan_search(c, nchain, k_learn_step<3, 1>, k_learn_step<4, 1>);
+    const SearchPlan P = c->retain > 1
+                             ? plan_search(c, nchain, k_learn_step<3, 4>, k_learn_step<4, 4>, k_learn_step<2, 4, 384>,
+                                           c->pack_w, c->pack_k)
+                             : plan_search(c, nchain, k_learn_step<3, 1>, k_learn_step<4, 1>, k_learn_step<2, 1, 384>,
+                                           c->pack_w, c->pack_k);
     c->best_floats = P.tot;
     c->d_best.ensure((size_t)P.tot);
     c->d_acc.ensure((size_t)P.tot);
@@ -1930,8 +1967,9 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     sp.p_learned = p_learned;
     sp.retain = c->retain;
     sp.nfeat_maps = std::min(c->nmaps, mlp::NMAP);
-    auto kern = c->retain > 1 ? (P.four ? k_learn_step<4, 4> : k_learn_step<3, 4>)
-                              : (P.four ? k_learn_step<4, 1> : k_learn_step<3, 1>);
+    auto kern = c->retain > 1
+                    ? (P.minb == 4 ? k_learn_step<4, 4> : (P.minb == 2 ? k_learn_step<2, 4, 384> : k_learn_step<3, 4>))
+                    : (P.minb == 4 ? k_learn_step<4, 1> : (P.minb == 2 ? k_learn_step<2, 1, 384> : k_learn_step<3, 1>));
     const int fblocks = (int)std::min<long long>((nch * 32 + 255) / 256, (long long)c->nsm * 16);
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -2255,6 +2293,24 @@ int ud_set_autotune(ud_ctx* c, int on) {
     if (!c) { g_err = "null context"; return UD_EINVAL; }
     c->autotune = on ? 1 : 0;
     c->tune_key = -1;
+    return UD_OK;
+}
+
+int ud_set_packing(ud_ctx* c, int warps_per_cta, int chains_per_warp) {
+    if (!c) { g_err = "null context"; return UD_EINVAL; }
+    if (!(warps_per_cta == 0 || warps_per_cta == 4 || warps_per_cta == 8 || warps_per_cta == 12) ||
+        chains_per_warp < 0 || chains_per_warp > 4) {
+        g_err = "packing: warps per CTA 0, 4, 8 or 12; chains per warp 0..4";
+        return UD_EINVAL;
+    }
+    c->pack_w = warps_per_cta;
+    c->pack_k = chains_per_warp;
+    return UD_OK;
+}
+
+int ud_search_shape(const ud_ctx* c, int* out4) {
+    if (!c || !out4) { g_err = "invalid arguments"; return UD_EINVAL; }
+    for (int i = 0; i < 4; i++) out4[i] = c->shape[i];
     return UD_OK;
 }
 

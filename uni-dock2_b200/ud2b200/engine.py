@@ -77,6 +77,8 @@ def load_library() -> C.CDLL:
         "ud_stage_times": ([vp, fp], i),
         "ud_counters": ([vp, ip], i),
         "ud_set_autotune": ([vp, i], i),
+        "ud_set_packing": ([vp, i, i], i),
+        "ud_search_shape": ([vp, ip], i),
         "ud_set_retain": ([vp, i], i),
         "ud_mlp_param_count": ([], C.c_longlong),
         "ud_mlp_init": ([vp, C.c_uint64], i),
@@ -298,6 +300,18 @@ class Engine:
     def set_autotune(self, on: bool = True):
         """Time chain packings on each new batch shape and keep the fastest (results unchanged)."""
         self._check(self.L.ud_set_autotune(self.h, int(bool(on))))
+
+    def set_packing(self, warps_per_cta: int = 0, chains_per_warp: int = 0):
+        """Fix the chain packing (4, 8 or 12 warps per CTA; 1..4 chains per warp per item;
+        0 = chosen per batch).  Results do not depend on it."""
+        self._check(self.L.ud_set_packing(self.h, int(warps_per_cta), int(chains_per_warp)))
+
+    def search_shape(self) -> dict:
+        """Launch shape of the last search."""
+        s = np.zeros(4, np.int32)
+        self._check(self.L.ud_search_shape(self.h, _p(s)))
+        return dict(warps_per_cta=int(s[0]), ctas_per_sm=int(s[1]), register_class=int(s[2]),
+                    chains_per_warp=int(s[3]))
 
     # ------------------------------------------------------------------ learned proposal
     MLP_IN, MLP_OUT, MLP_NDIM = 672, 64, 26
