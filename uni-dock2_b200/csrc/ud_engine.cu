@@ -1805,12 +1805,13 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, K k12, int want
     set_smem(chosen, P.smem);      // the candidates may have set a smaller size on the same kernel
     if (per_sm < 1) per_sm = 1;
     const long long resident = (long long)c->nsm * per_sm;
-    // k chains per warp per item (W*k chains): the warps of a CTA share an item's chains
-    // dynamically, so the wait at the item's end for its slowest chain shrinks with k;
-    // k stays small enough that every resident CTA gets at least two items
+    // k chains per warp per item (W*k chains; the warps of a CTA share an item's chains
+    // dynamically): one by default.  Larger items shorten the wait at an item's end relative
+    // to its length but lengthen the launch's tail; on a 148-ligand screen batch (12-warp
+    // CTAs, 400 MC steps) the search took 5.65 s at k = 1, 5.81 s at 2, 5.9-6.1 s at 3 and
+    // 5.8-6.3 s at 4.  The autotuner and ud_set_packing can choose others.
     const long long total_chains = (long long)nlig * nchain;
-    const int k = force_k > 0 ? force_k
-                              : (int)std::max(1LL, std::min(4LL, total_chains / std::max(1LL, 2 * resident * P.W)));
+    const int k = force_k > 0 ? force_k : 1;
     const int item_chains = P.W * k;
     std::vector<int4> items;
     for (int l : order)
