@@ -92,10 +92,11 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
-    """DRAM bytes (read + write) of one k_search launch at the default batch, from the
-    committed ncu summary of that launch."""
-    p = os.path.join(ROOT, "profiles", "k_search_screen.md")
+def load_traffic(summary: str = "k_search_screen.md"):
+    """DRAM bytes (read + write) of one launch of the dominant kernel at the default batch
+    (k_search, or k_learn_step: one MC step of every chain), from the committed ncu
+    summary of that launch."""
+    p = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -481,9 +482,12 @@ def run_ours(a):
     peak, peak_kind = load_peaks()
     bytes_alg = heavy * 8 * (2 if a.grid == "f16" else 4)
     achieved = bytes_alg / (search_ms / 1000.0) / 1e9 if search_ms > 0 else 0.0
-    tr = load_traffic()
-    traffic = tr if (tr is not None and not learned and nl == 148 and mc == w["mc_steps"] and a.workload == "screen") \
-        else None
+    # launches of the dominant kernel per step: k_search runs a dock's search in one launch,
+    # k_learn_step one MC step of every chain per launch
+    launches_per_step = run_kw["mc_steps"] if learned else 1
+    tr = load_traffic("k_learn_step_screen.md" if learned else "k_search_screen.md")
+    traffic = tr if (tr is not None and nl == 148 and a.workload == "screen" and a.grid == "f32"
+                     and (learned or mc == w["mc_steps"])) else None
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": tot_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic",
@@ -499,7 +503,8 @@ def run_ours(a):
                         "frac": achieved / peak, "traffic": traffic,
                         "kernel": "k_learn_step" if learned else "k_search",
                         "peak_kind": f"{peak_kind} hbm copy bandwidth",
-                        "algorithmic_bytes_per_launch": bytes_alg / a.steps},
+                        "algorithmic_bytes_per_launch": bytes_alg / a.steps / launches_per_step,
+                        "launches_per_step": launches_per_step},
            "e2e": {"value": ligs_done / tot_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
            "gpu_launches": launches,
            "stage_ms_per_step": [sum(x[i] for x in stage) / a.steps for i in range(6)],
