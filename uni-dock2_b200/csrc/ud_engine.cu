@@ -1926,11 +1926,16 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     for (const LigHost& h : c->h_ligs)
         if (h.natom > mlp::NATOM || h.ntors > mlp::TMAX)
             throw Fail(UD_EINVAL, "the proposal network covers ligands of at most 80 atoms and 20 torsions");
+    // two chains per warp per work item unless fixed: a launch runs one MC step of every
+    // chain, whose lengths vary far more than those of whole chains, and sharing an item's
+    // chains among its warps evens them out (148-ligand screen batch, 200 steps, p_learned
+    // 0.25: 2.46 s at k = 2, 2.58 s at 1, 2.56 s at 3, 2.73 s at 4)
+    const int lk = c->pack_k ? c->pack_k : 2;
     const SearchPlan P = c->retain > 1
                              ? plan_search(c, nchain, k_learn_step<3, 4>, k_learn_step<4, 4>, k_learn_step<2, 4, 384>,
-                                           c->pack_w, c->pack_k)
+                                           c->pack_w, lk)
                              : plan_search(c, nchain, k_learn_step<3, 1>, k_learn_step<4, 1>, k_learn_step<2, 1, 384>,
-                                           c->pack_w, c->pack_k);
+                                           c->pack_w, lk);
     c->best_floats = P.tot;
     c->d_best.ensure((size_t)P.tot);
     c->d_acc.ensure((size_t)P.tot);
