@@ -905,25 +905,27 @@ __device__ __forceinline__ void minus_hv(const double* H, const float* v, float*
     __syncwarp();
 }
 
-// Backtracking Armijo line search (bfgs.cuh:623-670).  Trial poses go to Pn.  init: only
-// evaluate Px (energy, gradient into W.g) -- the start of a BFGS run, taken through the
-// same evaluation call site as the trials so that the search loop holds one copy of the
-// evaluation code (4 % less search time than a separate call).
+constexpr int LS_TRIALS = 0, LS_INIT = 1, LS_MOVE = 2;
+// Backtracking Armijo line search (bfgs.cuh:623-670).  Trial poses go to Pn.  The start of a
+// BFGS run goes through the same call sites, so that the search loop holds one copy of the
+// evaluation and kinematics code: mode LS_INIT only evaluates Px (energy, gradient into
+// W.g); LS_MOVE sets Pn = Px moved by W.p (a learned MC move) and evaluates Pn likewise.
 __device__ UD_LS_ATTR float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, const Work& W,
                                              int dim, float e0, float vcap, float slope, float& alpha_out,
-                                             int& n_eval, bool init) {
+                                             int& n_eval, int mode) {
+    const bool start = mode != LS_TRIALS;
     float alpha = 1.f, e_new = 0.f;
-    const float pg = init ? 0.f : gdot(W.p, W.g, dim);
+    const float pg = start ? 0.f : gdot(W.p, W.g, dim);
 #pragma unroll 1
     for (int trial = 0; trial < LS_STEPS; trial++) {
-        if (!init) {
+        if (mode != LS_INIT) {
             slot_copy(Pn, Px, T.natom, T.ntors);
             apply_update(T, env, Pn, W.p, alpha, W.sc);
         }
-        const Slot Q = init ? Px : Pn;
-        e_new = eval_e_grad(T, env, Q, W.F, init ? W.g : W.gn, vcap, slope, W.pb);
+        const Slot Q = mode == LS_INIT ? Px : Pn;
+        e_new = eval_e_grad(T, env, Q, W.F, start ? W.g : W.gn, vcap, slope, W.pb);
         n_eval++;
-        if (init || e_new - e0 < 1e-4f * alpha * pg) break;
+        if (start || e_new - e0 < 1e-4f * alpha * pg) break;
         alpha *= 0.5f;
     }
     alpha_out = alpha;
@@ -933,21 +935,24 @@ __device__ UD_LS_ATTR float line_search(const Topo& T, const Env& env, Slot Px, 
 // BFGS on the pose in slot ix (bfgs.cuh:729-829).  Uses slots ix / ialt / iori; returns
 // the slot index holding the result, whose header[0] is the final energy.
 __device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots, int stride, int ix, int ialt,
-                                    int iori, const Work& W, int max_steps, float vcap, float slope, int& n_eval) {
+                                    int iori, const Work& W, int max_steps, float vcap, float slope, int& n_eval,
+                                    int move_from = -1) {
     const int lane = lane_id();
     const int dim = 6 + T.ntors;
     const Slot X = slot_at(slots, stride, ix, T.natom);
     float E_ori = 0.f, E = 0.f;
     const int ntri = dim * (dim + 1) / 2;
     int cur = ix, alt = ialt;
-    // step -1 evaluates the start pose (line_search with init) and sets H = I
+    // step -1 evaluates the start pose and sets H = I; move_from >= 0: the start pose is
+    // that slot moved by W.p (line_search LS_MOVE)
 #pragma unroll 1
     for (int step = -1; step < max_steps; step++) {
         if (step >= 0) minus_hv(W.H, W.g, W.p, dim);          // p = -H g
         float alpha;
-        const float E1 = line_search(T, env, slot_at(slots, stride, cur, T.natom),
-                                     slot_at(slots, stride, alt, T.natom), W, dim, E, vcap, slope, alpha, n_eval,
-                                     step < 0);
+        const bool mv = step < 0 && move_from >= 0;
+        const float E1 = line_search(T, env, slot_at(slots, stride, mv ? move_from : cur, T.natom),
+                                     slot_at(slots, stride, mv ? cur : alt, T.natom), W, dim, E, vcap, slope, alpha,
+                                     n_eval, step < 0 ? (mv ? LS_MOVE : LS_INIT) : LS_TRIALS);
         if (step < 0) {
             E_ori = E = E1;
 #pragma unroll 1

@@ -479,7 +479,8 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
             W.p[lane] = m;
         }
         __syncwarp();
-        apply_update(T, env, SC, W.p, 1.f, W.sc);
+        // with BFGS the move is applied by its first line-search call (LS_MOVE)
+        if (opt_steps == 0) apply_update(T, env, SC, W.p, 1.f, W.sc);
     } else {
         mutate(T, env, rng, (uint32_t)step, SC);
     }
@@ -504,7 +505,7 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
     for (int phase = 0; phase < 2; phase++) {
         const int X = (A + 1 - phase) & 3;
         const int R = bfgs(T, env, ws, stride, X, (X + 1) & 3, (X + 2) & 3, W, opt_steps,
-                           phase ? VCAP_AUTH : VCAP_SEARCH, PENALTY_SLOPE, ne);
+                           phase ? VCAP_AUTH : VCAP_SEARCH, PENALTY_SLOPE, ne, (phase == 0 && learned) ? A : -1);
         const float e_new = ws[R * stride];
         if (phase == 0) {
             if (!(step == 0 || metropolis(e_acc, e_new, 1.2f, rx))) break;
