@@ -236,7 +236,9 @@ int ud_set_autotune(ud_ctx* ctx, int on);
 
 /* Fixed chain packing for the searches of this context: warps per CTA (4, 8 or 12; 0 =
  * chosen per batch) and chains per warp per work item (1..4; 0 = chosen per batch).  Takes
- * precedence over the autotuner.  Results do not depend on the packing.
+ * precedence over the autotuner; a width whose CTA does not fit the shared memory falls back
+ * to the widest of at most 4 warps that fits (ud_search_shape reports what ran).  Results do
+ * not depend on the packing.
  * No reference counterpart. */
 int ud_set_packing(ud_ctx* ctx, int warps_per_cta, int chains_per_warp);
 
