@@ -226,3 +226,15 @@ def test_json_writer_layout(tmp_path, small_system):
                    ",".join(_fmt(F(x * RAD2DEG_F)) for x in rec[8 + n3:8 + n3 + lig.ntors]) +
                    '],"decomp":[' + ",".join("[" + ",".join(_fmt(x) for x in a) + "]" for a in r.decomp[j]) + "]}")
             assert exp in text, (lig.name, j)
+
+
+def test_bench_contract_helpers():
+    """bench.py's metric is the headline metric of the benchmark definition, and the per-launch
+    DRAM traffic it reports comes from the committed ncu summaries of both dominant kernels."""
+    import bench
+    with open(os.path.join(ROOT, "BASELINE.json")) as f:
+        assert bench.METRIC == json.load(f)["metric"]
+    assert bench.load_traffic("k_search_screen.md") == 12984320.0
+    assert bench.load_traffic("k_learn_step_screen.md") == 24054400.0
+    peak, kind = bench.load_peaks()
+    assert peak > 1000.0 and kind in ("measured", "fallback")
