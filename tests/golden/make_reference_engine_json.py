@@ -1,0 +1,46 @@
+"""Writes tests/golden/ref_engine_small_<batch>.json: the output files of the reference's own CUDA engine
+(core_pipeline, built from its sources into oracle/_ref/udref_dock by `make -C oracle refengine`)
+for the small test system (the `small_system` fixture of tests/conftest.py: 600-atom synthetic
+receptor, five ligands of 8-41 atoms) at 32 chains x 20 MC steps.  Needs a GPU and the built
+udref_dock; the CPU tests read the committed files (one per size-group batch the reference
+makes, src/screening/screening.cpp:17-41).
+
+    python tests/golden/make_reference_engine_json.py [out_dir]
+"""
+import glob
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "uni-dock2_b200"))
+
+
+def main(out_dir):
+    from ud2b200 import synth
+    rows, center = synth.make_receptor(600, 28.0, seed=3)
+    ligd = {f"l{i}": synth.make_ligand(n, t, seed=100 + i, center=center)
+            for i, (n, t) in enumerate([(8, 0), (14, 2), (20, 4), (30, 6), (41, 9)])}
+    exe = os.path.join(ROOT, "oracle", "_ref", "udref_dock")
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "input.json")
+        with open(inp, "w") as f:
+            json.dump(dict(receptor=rows, **ligd), f)
+        out = os.path.join(tmp, "out")
+        os.makedirs(out)
+        c = [str(float(v)) for v in center]
+        cmd = [exe, inp, out, *c, "20.0", "20.0", "20.0", "32", "20", "14", "2", "4", "1.0", "10.0", "5", "0"]
+        subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=600)
+        files = sorted(glob.glob(os.path.join(out, "udref_*.json")))
+        assert files
+        for fp in files:
+            batch = os.path.basename(fp)[len("udref_"):]
+            with open(fp) as src, open(os.path.join(out_dir, "ref_engine_small_" + batch), "w") as dst:
+                dst.write(src.read())
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
