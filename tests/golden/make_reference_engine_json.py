@@ -1,4 +1,5 @@
-"""Writes tests/golden/ref_engine_small_<batch>.json: the output files of the reference's own CUDA engine
+"""Writes tests/golden/ref_engine_small_<batch>.json and ref_engine_small_decomp_<batch>.json
+(energy_decomp on): the output files of the reference's own CUDA engine
 (core_pipeline, built from its sources into oracle/_ref/udref_dock by `make -C oracle refengine`)
 for the small test system (the `small_system` fixture of tests/conftest.py: 600-atom synthetic
 receptor, five ligands of 8-41 atoms) at 32 chains x 20 MC steps.  Needs a GPU and the built
@@ -29,17 +30,20 @@ def main(out_dir):
         inp = os.path.join(tmp, "input.json")
         with open(inp, "w") as f:
             json.dump(dict(receptor=rows, **ligd), f)
-        out = os.path.join(tmp, "out")
-        os.makedirs(out)
         c = [str(float(v)) for v in center]
-        cmd = [exe, inp, out, *c, "20.0", "20.0", "20.0", "32", "20", "14", "2", "4", "1.0", "10.0", "5", "0"]
-        subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=600)
-        files = sorted(glob.glob(os.path.join(out, "udref_*.json")))
-        assert files
-        for fp in files:
-            batch = os.path.basename(fp)[len("udref_"):]
-            with open(fp) as src, open(os.path.join(out_dir, "ref_engine_small_" + batch), "w") as dst:
-                dst.write(src.read())
+        # plain, and with energy_decomp (per-atom inter energy terms in the output)
+        for decomp, prefix in ((0, "ref_engine_small_"), (1, "ref_engine_small_decomp_")):
+            out = os.path.join(tmp, f"out{decomp}")
+            os.makedirs(out)
+            cmd = [exe, inp, out, *c, "20.0", "20.0", "20.0", "32", "20", "14", "2", "4", "1.0", "10.0", "5", "0",
+                   str(decomp)]
+            subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=600)
+            files = sorted(glob.glob(os.path.join(out, "udref_*.json")))
+            assert files
+            for fp in files:
+                batch = os.path.basename(fp)[len("udref_"):]
+                with open(fp) as src, open(os.path.join(out_dir, prefix + batch), "w") as dst:
+                    dst.write(src.read())
 
 
 if __name__ == "__main__":
