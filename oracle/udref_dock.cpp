@@ -5,7 +5,8 @@
 // own CUDA engine on the same GPU as this engine; nothing of the product calls it.
 //
 //   udref_dock input.json out_dir cx cy cz sx sy sz exhaustiveness mc_steps opt_steps
-//              refine_steps num_pose rmsd_limit energy_range seed constraint [energy_decomp]
+//              refine_steps num_pose rmsd_limit energy_range seed constraint
+//              [energy_decomp [bias bias_k]]      (bias: no | pos | align)
 //
 // Prints one JSON line: {"rc", "ligands", "seconds"} (wall time of core_pipeline).
 #include <chrono>
@@ -19,10 +20,10 @@
 #include "screening/core.h"
 
 int main(int argc, char** argv) {
-    if (argc != 18 && argc != 19) {
+    if (argc != 18 && argc != 19 && argc != 21) {
         std::fprintf(stderr, "usage: udref_dock input.json out_dir cx cy cz sx sy sz exhaustiveness mc_steps "
                              "opt_steps refine_steps num_pose rmsd_limit energy_range seed constraint "
-                             "[energy_decomp]\n");
+                             "[energy_decomp [bias bias_k]]\n");
         return 2;
     }
     std::ifstream f(argv[1]);
@@ -47,7 +48,11 @@ int main(int argc, char** argv) {
     ipt.energy_range = std::atof(argv[15]);
     ipt.seed = std::atoi(argv[16]);
     ipt.constraint_docking = std::atoi(argv[17]) != 0;
-    ipt.energy_decomp = argc == 19 && std::atoi(argv[18]) != 0;
+    ipt.energy_decomp = argc >= 19 && std::atoi(argv[18]) != 0;
+    if (argc == 21) {
+        ipt.bias = argv[19];
+        ipt.bias_k = std::atof(argv[20]);
+    }
     ipt.randomize = true;
     read_ud_from_json_string(ss.str(), ipt.box, ipt.fix_mol, ipt.flex_mol_list, ipt.fns_flex, false);
     const size_t nlig = ipt.flex_mol_list.size();

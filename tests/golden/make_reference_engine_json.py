@@ -1,5 +1,6 @@
-"""Writes tests/golden/ref_engine_small_<batch>.json and ref_engine_small_decomp_<batch>.json
-(energy_decomp on): the output files of the reference's own CUDA engine
+"""Writes tests/golden/ref_engine_small_<batch>.json, and ref_engine_small_decomp_ /
+_constraint_ / _bias_<batch>.json (energy_decomp on; constraint docking; positional bias
+records, k = 0.5): the output files of the reference's own CUDA engine
 (core_pipeline, built from its sources into oracle/_ref/udref_dock by `make -C oracle refengine`)
 for the small test system (the `small_system` fixture of tests/conftest.py: 600-atom synthetic
 receptor, five ligands of 8-41 atoms) at 32 chains x 20 MC steps.  Needs a GPU and the built
@@ -20,6 +21,24 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "uni-dock2_b200"))
 
 
+def bias_ligands(ligd):
+    """The ligands with positional bias records ([x, y, z, V, r2] per atom, the input schema's
+    optional 9th atom field) on every third atom, two on every sixth (seeded)."""
+    import copy
+    import numpy as np
+    rng = np.random.default_rng(17)
+    out = copy.deepcopy(ligd)
+    for lig in out.values():
+        for k, atom in enumerate(lig["atoms"]):
+            if k % 3 == 0:
+                recs = [[atom[0] + float(rng.uniform(-1, 1)), atom[1] + float(rng.uniform(-1, 1)),
+                         atom[2] + float(rng.uniform(-1, 1)), float(rng.uniform(-2, 2)), float(rng.uniform(0.5, 3.0))]]
+                if k % 6 == 0:
+                    recs.append([atom[0], atom[1] + 0.5, atom[2], -1.0, 1.5])
+                atom[:] = list(atom[:8]) + [recs]
+    return out
+
+
 def main(out_dir):
     from ud2b200 import synth
     rows, center = synth.make_receptor(600, 28.0, seed=3)
@@ -30,13 +49,20 @@ def main(out_dir):
         inp = os.path.join(tmp, "input.json")
         with open(inp, "w") as f:
             json.dump(dict(receptor=rows, **ligd), f)
+        inp_bias = os.path.join(tmp, "input_bias.json")
+        with open(inp_bias, "w") as f:
+            json.dump(dict(receptor=rows, **bias_ligands(ligd)), f)
         c = [str(float(v)) for v in center]
-        # plain, and with energy_decomp (per-atom inter energy terms in the output)
-        for decomp, prefix in ((0, "ref_engine_small_"), (1, "ref_engine_small_decomp_")):
-            out = os.path.join(tmp, f"out{decomp}")
+        # (input, constraint, extra arguments, output prefix): plain; energy_decomp (per-atom
+        # inter energy terms in the output); constraint docking; positional bias (k = 0.5)
+        runs = ((inp, "0", ["0"], "ref_engine_small_"), (inp, "0", ["1"], "ref_engine_small_decomp_"),
+                (inp, "1", ["0"], "ref_engine_small_constraint_"),
+                (inp_bias, "0", ["0", "pos", "0.5"], "ref_engine_small_bias_"))
+        for k, (src_in, constraint, extra, prefix) in enumerate(runs):
+            out = os.path.join(tmp, f"out{k}")
             os.makedirs(out)
-            cmd = [exe, inp, out, *c, "20.0", "20.0", "20.0", "32", "20", "14", "2", "4", "1.0", "10.0", "5", "0",
-                   str(decomp)]
+            cmd = [exe, src_in, out, *c, "20.0", "20.0", "20.0", "32", "20", "14", "2", "4", "1.0", "10.0", "5",
+                   constraint, *extra]
             subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=600)
             files = sorted(glob.glob(os.path.join(out, "udref_*.json")))
             assert files

@@ -171,3 +171,74 @@ def test_reference_decomposition_is_stale_after_the_first_batch():
     assert list(second) == ["l4"]
     for j, p in enumerate(second["l4"]):
         assert p["decomp"][:8] == first["l0"][j]["decomp"]
+
+
+CONSTRAINT_FILES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_engine_small_constraint_*.json")))
+BIAS_FILES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_engine_small_bias_*.json")))
+
+
+def test_constraint_docking_output_keeps_root_atoms(small_system):
+    """constraint_docking (no translation or rotation, src/cuda/mc.cu:159-166): every atom that
+    no torsion moves keeps its input coordinates in every pose the reference engine printed --
+    the semantics this build's constraint docking follows (its GPU test checks the same)."""
+    from unidock_engine.api.python.pipeline import _fmt
+    assert CONSTRAINT_FILES
+    ligs = small_system["ligs"]
+    n = 0
+    for name, poses in _poses(CONSTRAINT_FILES).items():
+        lig = ligs[int(name[1:])]
+        moved = np.zeros(lig.natom, bool)
+        for r in lig.rotated:
+            moved[r] = True
+        root = np.where(~moved)[0]
+        want = [float(_fmt(np.float32(v))) for v in lig.coords[root].reshape(-1)]
+        for p in poses:
+            assert np.asarray(p["coords"]).reshape(-1, 3)[root].reshape(-1).tolist() == want, name
+            n += 1
+    assert n >= 5
+
+
+def test_bias_output_matches_reference_host_score_and_oracle(small_system, oracle64):
+    """bias = 'pos', bias_k = 0.5 with positional bias records: the printed intra, inter,
+    penalty and bias (energy[6]) against the reference's host score() with the same records
+    and the FP64 oracle, on the printed coordinates."""
+    import ctypes as C
+    import importlib.util
+    from ud2b200.model import parse_ligands
+    assert BIAS_FILES
+    spec = importlib.util.spec_from_file_location("mkref", os.path.join(HERE, "golden", "make_reference_engine_json.py"))
+    mkref = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mkref)
+    ligs = parse_ligands(mkref.bias_ligands(small_system["ligd"]))
+    rec, box = small_system["rec"], small_system["box"]
+    env = oracle64.make_env(rec, box, mode="direct", bias_type=1, bias_k=0.5)
+    ref = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libudref_f64.so")
+    R = C.CDLL(ref) if os.path.exists(ref) else None
+    rx = rec.xyz.astype(np.float64).reshape(-1)
+    b6 = box.as6().astype(np.float64)
+    worst, nonzero = 0.0, 0
+    for name, poses in _poses(BIAS_FILES).items():
+        lig = ligs[int(name[1:])]
+        assert lig.bias_atoms.size > 0
+        ba = np.ascontiguousarray(lig.bias_atoms.astype(np.int32))
+        bp = np.ascontiguousarray(lig.bias_params.astype(np.float64).reshape(-1))
+        for p in poses:
+            x = np.asarray(p["coords"], np.float64)
+            e = p["energy"]
+            printed = np.array([e[2], e[3], e[4], e[6]])
+            want = np.asarray(oracle64.score_terms(oracle64.ligand(lig), env, x.reshape(-1, 3)), np.float64)
+            if R is not None:
+                out4 = np.zeros(4)
+                R.udref_score(C.c_int(lig.natom), x.ctypes.data_as(C.c_void_p), lig.types.ctypes.data_as(C.c_void_p),
+                              lig.pair_off.ctypes.data_as(C.c_void_p), lig.pairs.ctypes.data_as(C.c_void_p),
+                              C.c_int(rec.natom), rx.ctypes.data_as(C.c_void_p), rec.types.ctypes.data_as(C.c_void_p),
+                              b6.ctypes.data_as(C.c_void_p), C.c_int(1), C.c_double(0.5), C.c_int(ba.size),
+                              ba.ctypes.data_as(C.c_void_p), bp.ctypes.data_as(C.c_void_p),
+                              out4.ctypes.data_as(C.c_void_p))
+                assert np.allclose(out4, want, rtol=1e-6, atol=1e-6), (name, out4, want)
+            err = np.abs(printed - want)
+            worst = max(worst, float(err.max()))
+            nonzero += abs(e[6]) > 1e-3
+            assert np.all(err <= 0.02 + 2e-3 * np.abs(want)), (name, printed, want)
+    assert nonzero >= 5
+    print(f"printed vs recomputed terms with bias: max |d| {worst:.2e} kcal/mol")
