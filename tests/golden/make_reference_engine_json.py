@@ -1,6 +1,7 @@
 """Writes tests/golden/ref_engine_small_<batch>.json, and ref_engine_small_decomp_ /
-_constraint_ / _bias_<batch>.json (energy_decomp on; constraint docking; positional bias
-records, k = 0.5): the output files of the reference's own CUDA engine
+_constraint_ / _bias_ / _align_<batch>.json (energy_decomp on; constraint docking; bias records
+with bias 'pos', k = 0.5, and 'align', k = 0.1): the output files of the reference's own CUDA
+engine
 (core_pipeline, built from its sources into oracle/_ref/udref_dock by `make -C oracle refengine`)
 for the small test system (the `small_system` fixture of tests/conftest.py: 600-atom synthetic
 receptor, five ligands of 8-41 atoms) at 32 chains x 20 MC steps.  Needs a GPU and the built
@@ -54,10 +55,12 @@ def main(out_dir):
             json.dump(dict(receptor=rows, **bias_ligands(ligd)), f)
         c = [str(float(v)) for v in center]
         # (input, constraint, extra arguments, output prefix): plain; energy_decomp (per-atom
-        # inter energy terms in the output); constraint docking; positional bias (k = 0.5)
+        # inter energy terms in the output); constraint docking; positional bias (k = 0.5);
+        # z-align bias (k = 0.1)
         runs = ((inp, "0", ["0"], "ref_engine_small_"), (inp, "0", ["1"], "ref_engine_small_decomp_"),
                 (inp, "1", ["0"], "ref_engine_small_constraint_"),
-                (inp_bias, "0", ["0", "pos", "0.5"], "ref_engine_small_bias_"))
+                (inp_bias, "0", ["0", "pos", "0.5"], "ref_engine_small_bias_"),
+                (inp_bias, "0", ["0", "align", "0.1"], "ref_engine_small_align_"))
         for k, (src_in, constraint, extra, prefix) in enumerate(runs):
             out = os.path.join(tmp, f"out{k}")
             os.makedirs(out)

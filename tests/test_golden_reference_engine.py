@@ -175,6 +175,7 @@ def test_reference_decomposition_is_stale_after_the_first_batch():
 
 CONSTRAINT_FILES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_engine_small_constraint_*.json")))
 BIAS_FILES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_engine_small_bias_*.json")))
+ALIGN_FILES = sorted(glob.glob(os.path.join(HERE, "golden", "ref_engine_small_align_*.json")))
 
 
 def test_constraint_docking_output_keeps_root_atoms(small_system):
@@ -198,26 +199,28 @@ def test_constraint_docking_output_keeps_root_atoms(small_system):
     assert n >= 5
 
 
-def test_bias_output_matches_reference_host_score_and_oracle(small_system, oracle64):
-    """bias = 'pos', bias_k = 0.5 with positional bias records: the printed intra, inter,
-    penalty and bias (energy[6]) against the reference's host score() with the same records
-    and the FP64 oracle, on the printed coordinates."""
+@pytest.mark.parametrize("kind", ["pos", "align"])
+def test_bias_output_matches_reference_host_score_and_oracle(small_system, oracle64, kind):
+    """bias = 'pos' (k 0.5) and 'align' (k 0.1) with bias records on every third atom: the
+    printed intra, inter, penalty and bias (energy[6]) against the reference's host score()
+    with the same records and the FP64 oracle, on the printed coordinates."""
+    files, bias_type, bias_k = (BIAS_FILES, 1, 0.5) if kind == "pos" else (ALIGN_FILES, 2, 0.1)
     import ctypes as C
     import importlib.util
     from ud2b200.model import parse_ligands
-    assert BIAS_FILES
+    assert files
     spec = importlib.util.spec_from_file_location("mkref", os.path.join(HERE, "golden", "make_reference_engine_json.py"))
     mkref = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mkref)
     ligs = parse_ligands(mkref.bias_ligands(small_system["ligd"]))
     rec, box = small_system["rec"], small_system["box"]
-    env = oracle64.make_env(rec, box, mode="direct", bias_type=1, bias_k=0.5)
+    env = oracle64.make_env(rec, box, mode="direct", bias_type=bias_type, bias_k=bias_k)
     ref = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "libudref_f64.so")
     R = C.CDLL(ref) if os.path.exists(ref) else None
     rx = rec.xyz.astype(np.float64).reshape(-1)
     b6 = box.as6().astype(np.float64)
     worst, nonzero = 0.0, 0
-    for name, poses in _poses(BIAS_FILES).items():
+    for name, poses in _poses(files).items():
         lig = ligs[int(name[1:])]
         assert lig.bias_atoms.size > 0
         ba = np.ascontiguousarray(lig.bias_atoms.astype(np.int32))
@@ -232,7 +235,7 @@ def test_bias_output_matches_reference_host_score_and_oracle(small_system, oracl
                 R.udref_score(C.c_int(lig.natom), x.ctypes.data_as(C.c_void_p), lig.types.ctypes.data_as(C.c_void_p),
                               lig.pair_off.ctypes.data_as(C.c_void_p), lig.pairs.ctypes.data_as(C.c_void_p),
                               C.c_int(rec.natom), rx.ctypes.data_as(C.c_void_p), rec.types.ctypes.data_as(C.c_void_p),
-                              b6.ctypes.data_as(C.c_void_p), C.c_int(1), C.c_double(0.5), C.c_int(ba.size),
+                              b6.ctypes.data_as(C.c_void_p), C.c_int(bias_type), C.c_double(bias_k), C.c_int(ba.size),
                               ba.ctypes.data_as(C.c_void_p), bp.ctypes.data_as(C.c_void_p),
                               out4.ctypes.data_as(C.c_void_p))
                 assert np.allclose(out4, want, rtol=1e-6, atol=1e-6), (name, out4, want)
@@ -241,4 +244,4 @@ def test_bias_output_matches_reference_host_score_and_oracle(small_system, oracl
             nonzero += abs(e[6]) > 1e-3
             assert np.all(err <= 0.02 + 2e-3 * np.abs(want)), (name, printed, want)
     assert nonzero >= 5
-    print(f"printed vs recomputed terms with bias: max |d| {worst:.2e} kcal/mol")
+    print(f"printed vs recomputed terms with bias {kind}: max |d| {worst:.2e} kcal/mol")
