@@ -124,8 +124,12 @@ int ud_score_batch(ud_ctx* ctx, int n, const int* pose_lig, const float* coords,
  * - All contexts on a device share the one array: calls that overlap in time (from
  *   several threads, or several contexts on one device) race on it and must be
  *   serialised by the caller. */
+#ifndef UD_NOALLOC_MAX_POSES
 #define UD_NOALLOC_MAX_POSES 16384
+#endif
+#ifndef UD_NOALLOC_SCRATCH_BYTES
 #define UD_NOALLOC_SCRATCH_BYTES (8u << 20)
+#endif
 int ud_score_batch_noalloc(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, const float* centers,
                            const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g);
 

@@ -525,6 +525,10 @@ R orc_e_f(const orc_lig* lig, const orc_env* env, const orc_pose* pose, R vcap, 
             aux_f[3 * i] += fb[0]; aux_f[3 * i + 1] += fb[1]; aux_f[3 * i + 2] += fb[2];
         }
     }
+    /* A pose with a non-finite coordinate scores +inf (the engine's rule; the reference's
+       cutoff and box tests all fail on NaN and give such a pose a finite energy). */
+    for (int i = 0; i < 3 * n; i++)
+        if (!isfinite(X[i])) return (R)INFINITY;
     return energy;
 }
 

@@ -170,6 +170,50 @@ def test_collect_moves_and_learned_search(search_sys):
         assert np.all(np.isfinite(recs[:, 1:4])) and np.all(np.isfinite(recs[:, 8:8 + 3 * lig.natom]))
 
 
+@pytest.mark.parametrize("p_learned", [0.5, 1.0])
+def test_untrained_learned_search_keeps_every_pose_finite(search_sys, p_learned):
+    """An untrained network proposes large, arbitrary moves; the poses they lead to (some
+    far outside the box, where the penalty gradient drives BFGS steps that overflow) must
+    never reach a chain record or a docked pose: every record and every output pose has
+    finite energy, centre and coordinates."""
+    eng = search_sys["eng"]
+    ligs = search_sys["ligs"]
+    eng.mlp_init(17)
+    for seed in (41, 42):
+        eng.search_learned(seed=seed, nchain=32, mc_steps=12, opt_steps=5, p_learned=p_learned)
+        for li, lig in enumerate(ligs):
+            recs = eng.chain_poses(li)
+            assert np.all(np.isfinite(recs[:, 0])) and np.all(recs[:, 0] < 1e8), (seed, li)
+            assert np.all(np.isfinite(recs[:, 1:4])), (seed, li)
+            assert np.all(np.isfinite(recs[:, 8:8 + 3 * lig.natom + lig.ntors])), (seed, li)
+    res, _ = eng.dock(seed=43, nchain=16, mc_steps=8, opt_steps=4, refine_steps=2, num_pose=3, rmsd_limit=1.0,
+                      energy_range=10.0, p_learned=p_learned)
+    for r, lig in zip(res, ligs):
+        assert np.all(np.isfinite(r.terms))
+        for rec in r.records:
+            assert np.all(np.isfinite(rec[:4])) and np.all(np.isfinite(rec[8:8 + 3 * lig.natom]))
+
+
+@pytest.mark.parametrize("target", [0, 1])
+def test_move_recording_is_deterministic(search_sys, target):
+    """Recorded rows come in (step, chain) order, so two collections with the same seed give
+    the same training set, row for row."""
+    eng = search_sys["eng"]
+    sets = []
+    for _ in range(2):
+        n = eng.collect_moves(seed=7, nchain=24, mc_steps=10, opt_steps=4, max_moves=5000, target=target)
+        assert n > 0
+        sets.append(eng.get_moves(n))
+    for a, b in zip(sets[0], sets[1]):
+        assert np.array_equal(a, b)
+    # a cap below the count keeps the first rows of the same order
+    n = eng.collect_moves(seed=7, nchain=24, mc_steps=10, opt_steps=4, max_moves=50, target=target)
+    assert n == 50
+    x, y, m = eng.get_moves(n)
+    assert np.array_equal(x, sets[0][0][:50])
+    assert np.array_equal(y, sets[0][1][:50]) and np.array_equal(m, sets[0][2][:50])
+
+
 def test_collect_moves_to_ligand_best(search_sys):
     """Target 1: every recorded pose labelled with the move to its ligand's best pose."""
     eng = search_sys["eng"]

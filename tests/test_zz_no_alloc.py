@@ -47,6 +47,50 @@ def test_noalloc_matches_score_batch_twice(small_system, mode_name):
         eng.close()
 
 
+def test_noalloc_more_poses_than_one_scan_block(small_system):
+    """3000 poses: the offset prefix sums carry across 1024-pose blocks of the scan."""
+    from ud2b200 import MODE_GRID
+    eng, _ = engine_for(small_system)
+    try:
+        pl, xs, cs, rs = _poses(small_system, np.random.default_rng(11), 600)
+        order = np.random.default_rng(12).permutation(len(pl))        # ligands interleaved
+        pl = [pl[i] for i in order]
+        xs = [xs[i] for i in order]
+        cs, rs = cs[order], rs[order]
+        assert len(pl) == 3000
+        want_e, want_g = eng.score_batch(pl, xs, cs, rs, mode=MODE_GRID, vcap=10.0, slope=1e6)
+        for _ in range(2):
+            e, gs = eng.score_batch_noalloc(pl, xs, cs, rs, mode=MODE_GRID, vcap=10.0, slope=1e6)
+            np.testing.assert_allclose(e, want_e, rtol=TOL, atol=TOL)
+            for g, w in zip(gs, want_g):
+                np.testing.assert_allclose(g, w, rtol=TOL, atol=TOL)
+    finally:
+        eng.close()
+
+
+def test_noalloc_refuses_a_batch_whose_staging_exceeds_the_array(small_system):
+    """16000 poses of the 41-atom ligand: under the pose limit, but coordinates alone take
+    7.9 MB and the whole staging more than the fixed 8 MiB, so the call is refused with
+    UD_EINVAL before anything is copied; a smaller batch then still goes through."""
+    from ud2b200 import EngineError, MODE_GRID
+    eng, _ = engine_for(small_system)
+    try:
+        li = 4
+        lig = small_system["ligs"][li]
+        assert lig.natom == 41
+        pl, xs, cs, rs = _poses(small_system, np.random.default_rng(13), 4)
+        want_e, _ = eng.score_batch(pl, xs, cs, rs, mode=MODE_GRID)     # uploads the ligand set
+        n = 16000
+        x = np.zeros((lig.natom, 3), np.float32)
+        with pytest.raises(EngineError, match="bytes of staging"):
+            eng.score_batch_noalloc([li] * n, [x] * n, np.zeros((n, 3), np.float32), np.zeros((n, 3), np.float32),
+                                    mode=MODE_GRID)
+        e, _ = eng.score_batch_noalloc(pl, xs, cs, rs, mode=MODE_GRID)
+        np.testing.assert_allclose(e, want_e, rtol=TOL, atol=TOL)
+    finally:
+        eng.close()
+
+
 def test_noalloc_limits_and_state(small_system):
     from ud2b200 import EngineError, MODE_GRID
     from ud2b200.engine import load_library

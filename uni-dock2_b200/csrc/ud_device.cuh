@@ -610,15 +610,22 @@ __device__ __forceinline__ float intra_atomic(const Topo& T, const float* X, flo
 // ---------------------------------------------------------------- energy + force
 // Fills F (3N, dE/dx per atom) and returns the warp-summed energy (bfgs.cuh:221-394).
 // PB: the warp's pair buffer for ligands above 32 atoms (null: atomic accumulation).
+// A pose with a non-finite coordinate scores +inf.  In the reference such a pose (left by
+// a rotation increment whose norm overflows, quaternion.h:90-107 then gives sin(inf))
+// escapes every cutoff and box test and gets a finite energy, so Metropolis and the best
+// records could take it; +inf makes the line search, the BFGS revert, Metropolis and the
+// best records all reject it, and changes nothing for finite poses.
 __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* F, float vcap,
                                           float slope, float* PB) {
     const int lane = lane_id();
     float energy = 0.f;
+    bool bad = false;
     // inter + penalty
 #pragma unroll 1
     for (int i = lane; i < T.natom; i += WARP) {
         const int ti = T.type(i);
         float fx = 0.f, fy = 0.f, fz = 0.f;
+        bad |= !(isfinite(X[3 * i]) && isfinite(X[3 * i + 1]) && isfinite(X[3 * i + 2]));
         if (ti != VN_H) {
             const float px = X[3 * i], py = X[3 * i + 1], pz = X[3 * i + 2];
             float e_atom = 0.f;
@@ -699,7 +706,8 @@ __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const f
         }
     }
     __syncwarp();
-    return warp_sum(energy);
+    const float e = warp_sum(energy);
+    return __any_sync(FULL, bad) ? INFINITY : e;
 }
 
 // Generalised gradient from per-atom dE/dx (bfgs.cuh:69-193).  G has 6+ntors entries.

@@ -194,9 +194,6 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
 // module loads), shared by every context on that device.  Holds, 256-byte aligned in
 // this order: pose ligand ids (int), coordinate and gradient offsets (int64), coordinates,
 // centres, rotation vectors, energies and gradients (float).
-#ifndef UD_NOALLOC_SCRATCH_BYTES
-#define UD_NOALLOC_SCRATCH_BYTES (8u << 20)
-#endif
 static __device__ __align__(256) unsigned char g_noalloc_scratch[UD_NOALLOC_SCRATCH_BYTES];
 
 // exclusive prefix sums of 3*natom and 6+ntors over the poses (one CTA of 1024 threads)
@@ -618,6 +615,12 @@ struct MoveSet {              // recorded accepted moves (training data)
     int target;               // 0: the move to the next accepted pose; 1: to the ligand's best pose
     float* aux;               // target 1: [max][32] centre, rigid-frame atoms, dihedrals of the pose
     long long* chain;         // target 1: [max] chain of the sample
+    // per-chain staging of one step ([chain] rows); k_move_scan / k_move_copy append the
+    // staged rows in chain order, so the set's row order is (step, chain) on every run
+    int* sflag;               // [nch] 1: the chain recorded a move this step
+    int* spos;                // [nch] row in the set, or -1
+    float* sy;                // [nch][26] move (target 0) or [nch][32] pose (target 1)
+    float* sm;                // [nch][26] mask (target 0)
 };
 constexpr int AUX = 32;
 
@@ -710,12 +713,17 @@ __device__ void frame_rotvec(const float* xo, const float* xn, int f0, int f1, i
     frame_rotvec_pts(po, pn, rv);
 }
 
-// append (features before the move, the move, its mask) to the move set; moves with a
-// non-finite value (a chain whose pose diverged) are not recorded
-__device__ void record_move(const Topo& T, const Env& env, const float* old_rec, Slot P, const __nv_bfloat16* xrow,
-                            MoveSet D, long long g) {
+// stage (the move, its mask) of chain g for this step; the features of the pose before
+// the move are row g of the step's feature matrix.  Moves with a non-finite value (a chain
+// whose pose diverged) are not recorded.  Every chain writes its flag every step.
+__device__ void record_move(const Topo& T, const Env& env, const float* old_rec, Slot P, bool accepted, MoveSet D,
+                            long long g) {
     const int lane = lane_id();
     const int f0 = T.b[H_FRAME0], f1 = T.b[H_FRAME0 + 1], f2 = T.b[H_FRAME0 + 2];
+    if (!accepted) {
+        if (lane == 0) D.sflag[g] = 0;
+        return;
+    }
     if (D.target == 1) {
         // the pose before the move; its target is labelled after the run (k_label_moves)
         float a = 0.f;
@@ -723,16 +731,9 @@ __device__ void record_move(const Topo& T, const Env& env, const float* old_rec,
         else if (lane < 12) { const int j = (lane - 3) / 3, i = (lane - 3) % 3; const int f = j == 0 ? f0 : (j == 1 ? f1 : f2);
                               a = f >= 0 ? old_rec[8 + 3 * f + i] : 0.f; }
         else if (lane - 12 < T.ntors) a = old_rec[8 + 3 * T.natom + (lane - 12)];
-        if (!__all_sync(FULL, isfinite(a))) return;
-        int idx = 0;
-        if (lane == 0) idx = atomicAdd(D.count, 1);
-        idx = __shfl_sync(FULL, idx, 0);
-        if (idx >= D.max) return;
-        const uint32_t* xs = reinterpret_cast<const uint32_t*>(xrow);
-        uint32_t* xd = reinterpret_cast<uint32_t*>(D.x + (long long)idx * mlp::IN);
-        for (int i = lane; i < mlp::IN / 2; i += WARP) xd[i] = xs[i];
-        D.aux[(long long)idx * AUX + lane] = a;
-        if (lane == 0) D.chain[idx] = g;
+        const bool ok = __all_sync(FULL, isfinite(a));
+        D.sy[g * AUX + lane] = a;
+        if (lane == 0) D.sflag[g] = ok ? 1 : 0;
         return;
     }
     const bool rigid = !env.constraint;
@@ -753,17 +754,67 @@ __device__ void record_move(const Topo& T, const Env& env, const float* old_rec,
         yv = normalize_angle(P.d[lane - 6] - old_rec[8 + 3 * T.natom + (lane - 6)]);
         mv = 1.f;
     }
-    if (!__all_sync(FULL, isfinite(yv))) return;
-    int idx = 0;
-    if (lane == 0) idx = atomicAdd(D.count, 1);
-    idx = __shfl_sync(FULL, idx, 0);
-    if (idx >= D.max) return;
-    const uint32_t* xs = reinterpret_cast<const uint32_t*>(xrow);
-    uint32_t* xd = reinterpret_cast<uint32_t*>(D.x + (long long)idx * mlp::IN);
-    for (int i = lane; i < mlp::IN / 2; i += WARP) xd[i] = xs[i];
+    const bool ok = __all_sync(FULL, isfinite(yv));
     if (lane < mlp::NDIM) {
-        D.y[(long long)idx * mlp::NDIM + lane] = yv;
-        D.m[(long long)idx * mlp::NDIM + lane] = mv;
+        D.sy[g * mlp::NDIM + lane] = yv;
+        D.sm[g * mlp::NDIM + lane] = mv;
+    }
+    if (lane == 0) D.sflag[g] = ok ? 1 : 0;
+}
+
+// rows of the staged moves in chain order: spos[g] = count + (flags before g), or -1;
+// count += flags (one CTA of 1024 threads)
+__global__ void __launch_bounds__(1024) k_move_scan(MoveSet D, long long nch) {
+    __shared__ int sw[32];
+    __shared__ int carry;
+    const int warp = threadIdx.x >> 5, lane = lane_id();
+    if (threadIdx.x == 0) carry = *D.count;
+    __syncthreads();
+    for (long long base = 0; base < nch; base += blockDim.x) {
+        const long long g = base + threadIdx.x;
+        const int f = g < nch ? D.sflag[g] : 0;
+        int incl = f;
+        for (int d = 1; d < WARP; d <<= 1) {
+            const int t = __shfl_up_sync(FULL, incl, d);
+            if (lane >= d) incl += t;
+        }
+        if (lane == WARP - 1) sw[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int w = lane < (int)(blockDim.x >> 5) ? sw[lane] : 0;
+            for (int d = 1; d < WARP; d <<= 1) {
+                const int t = __shfl_up_sync(FULL, w, d);
+                if (lane >= d) w += t;
+            }
+            sw[lane] = w;
+        }
+        __syncthreads();
+        const int pre = carry + (warp ? sw[warp - 1] : 0) + incl - f;
+        if (g < nch) D.spos[g] = f ? pre : -1;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = pre + f;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *D.count = carry;
+}
+
+// copy each staged row to its place in the set (warp per chain; rows past max are dropped)
+__global__ void k_move_copy(MoveSet D, const __nv_bfloat16* __restrict__ X, long long nch) {
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int lane = lane_id();
+    for (long long g = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; g < nch; g += nw) {
+        const int idx = D.spos[g];
+        if (idx < 0 || idx >= D.max) continue;
+        const uint32_t* xs = reinterpret_cast<const uint32_t*>(X + g * mlp::IN);
+        uint32_t* xd = reinterpret_cast<uint32_t*>(D.x + (long long)idx * mlp::IN);
+        for (int i = lane; i < mlp::IN / 2; i += WARP) xd[i] = xs[i];
+        if (D.target == 1) {
+            D.aux[(long long)idx * AUX + lane] = D.sy[g * AUX + lane];
+            if (lane == 0) D.chain[idx] = g;
+        } else if (lane < mlp::NDIM) {
+            D.y[(long long)idx * mlp::NDIM + lane] = D.sy[g * mlp::NDIM + lane];
+            D.m[(long long)idx * mlp::NDIM + lane] = D.sm[g * mlp::NDIM + lane];
+        }
     }
 }
 
@@ -895,7 +946,7 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
             const int A = mc_step(T, env, ws, L.stride, 0, W, rng, step, sp.opt_steps, nrec, keep, ne, prop,
                                   accepted);
             const Slot SN = slot_at(ws, L.stride, A, T.natom);
-            if (rec_set.count && accepted && step > 0) record_move(T, env, accp, SN, X + g * mlp::IN, rec_set, g);
+            if (rec_set.count && step > 0) record_move(T, env, accp, SN, accepted, rec_set, g);
             __syncwarp();
             copy_words(accp, SN.h, nrec);
             my_evals += ne;
@@ -1125,6 +1176,8 @@ struct ud_ctx {
     DBuf<int> d_mcount, d_ligbest;
     DBuf<float> d_maux;
     DBuf<long long> d_mchain;
+    DBuf<int> d_sflag, d_spos;          // per-chain move staging of one learned-search step
+    DBuf<float> d_sy, d_sm;
     int moves_max = 0, moves_n = 0;
     // chain packing autotuner (warps per CTA, chains per warp per work item)
     int autotune = 0, tune_w = 8, tune_k = 0;
@@ -1946,7 +1999,7 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
         c->mlp.ensure((int)nch);
         c->mlp.prepare(c->stream);                  // nothing may allocate inside the capture
     }
-    MoveSet ms{nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr};
+    MoveSet ms{nullptr, nullptr, nullptr, nullptr, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (record_max > 0) {
         c->d_mx.ensure((size_t)record_max * mlp::IN);
         c->d_my.ensure((size_t)record_max * mlp::NDIM);
@@ -1956,9 +2009,15 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
             c->d_maux.ensure((size_t)record_max * AUX);
             c->d_mchain.ensure((size_t)record_max);
         }
+        c->d_sflag.ensure((size_t)nch);
+        c->d_spos.ensure((size_t)nch);
+        c->d_sy.ensure((size_t)nch * (target == 1 ? AUX : mlp::NDIM));
+        if (target == 0) c->d_sm.ensure((size_t)nch * mlp::NDIM);
         ck(cudaMemsetAsync(c->d_mcount.p, 0, sizeof(int), c->stream), "memset");
+        ck(cudaMemsetAsync(c->d_sflag.p, 0, sizeof(int) * (size_t)nch, c->stream), "memset");
         ms = MoveSet{c->d_mx.p, c->d_my.p, c->d_mm.p, c->d_mcount.p, record_max, target,
-                     target == 1 ? c->d_maux.p : nullptr, target == 1 ? c->d_mchain.p : nullptr};
+                     target == 1 ? c->d_maux.p : nullptr, target == 1 ? c->d_mchain.p : nullptr,
+                     c->d_sflag.p, c->d_spos.p, c->d_sy.p, target == 0 ? c->d_sm.p : nullptr};
         c->moves_max = record_max;
     }
     c->d_step.ensure(1);
@@ -1992,6 +2051,10 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
                                                       c->d_step.p, c->d_acc.p, c->d_best.p,
                                                       p_learned > 0.f ? c->mlp.out.p : nullptr, c->d_x16.p, ms,
                                                       c->d_counter.p, c->d_nevals.p);
+        if (record_max > 0) {
+            k_move_scan<<<1, 1024, 0, c->stream>>>(ms, nch);
+            k_move_copy<<<fblocks, 256, 0, c->stream>>>(ms, c->d_x16.p, nch);
+        }
         k_step_advance<<<1, 1, 0, c->stream>>>(c->d_step.p);
     } catch (...) {
         cudaStreamEndCapture(c->stream, &graph);
@@ -2009,7 +2072,7 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     ck(le, "graph launch");
     ck(se, "learned search");
     if (p_learned > 0.f) c->mlp.check_tc(c->stream);
-    c->counters[2] += (long long)mc_steps * (3 + (feats ? 1 : 0) + (p_learned > 0.f ? 4 : 0));
+    c->counters[2] += (long long)mc_steps * (3 + (feats ? 1 : 0) + (p_learned > 0.f ? 4 : 0) + (record_max > 0 ? 2 : 0));
 }
 
 static void read_search_counters(ud_ctx* c) {
@@ -2503,7 +2566,8 @@ int ud_collect_moves(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt
             const int nlig = (int)c->h_ligs.size();
             c->d_ligbest.ensure((size_t)nlig);
             k_lig_best<<<nlig, 256, 0, c->stream>>>(c->d_ligs.p, nlig, nchain, c->d_best.p, c->d_ligbest.p);
-            MoveSet ms{c->d_mx.p, c->d_my.p, c->d_mm.p, c->d_mcount.p, max_moves, 1, c->d_maux.p, c->d_mchain.p};
+            MoveSet ms{c->d_mx.p,    c->d_my.p,     c->d_mm.p, c->d_mcount.p, max_moves, 1,
+                       c->d_maux.p,  c->d_mchain.p, nullptr,   nullptr,        nullptr,   nullptr};
             const long long threads = (long long)*out_count * 32;
             k_label_moves<<<(unsigned)((threads + 255) / 256), 256, 0, c->stream>>>(
                 c->d_blobs.p, c->d_ligs.p, nchain, c->d_best.p, c->d_ligbest.p, ms, *out_count, c->constraint);
