@@ -23,6 +23,7 @@
 #ifndef UDOCK_B200_H
 #define UDOCK_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -40,6 +41,11 @@ int ud_version(void);
 
 /* Message of the last failing call on this thread ("" if none). */
 const char* ud_last_error(void);
+
+/* Free and total device memory of CUDA device `device`, in bytes (the budget of the
+ * memory-bounded batches when no max_gpu_mem is given).
+ * Replaces: the device-memory query of decide_memory_limit_mb (src/screening/core.cpp:32-63). */
+int ud_device_memory(int device, long long* out_free, long long* out_total);
 
 /* Create a context on CUDA device `device` for the docking box
  * box6 = {x_lo, x_hi, y_lo, y_hi, z_lo, z_hi}.
@@ -91,6 +97,31 @@ int ud_add_ligands(ud_ctx* ctx, int nlig, const int* atom_off, const float* xyz,
                    const int* tors_off, const int* axis, const float* dihedrals,
                    const int* range_off, const float* ranges, const int* rot_off, const int* rot_atoms,
                    const int* pair_off, const int* pairs, const int* bias_off, const float* bias);
+
+/* Bulk ligand input (host only, no GPU needed).  Parses a JSON document in the engine's
+ * ligand schema (an object of ligands; the reserved keys "receptor" and "score" are
+ * skipped) and builds, for every ligand, the 1-2/1-3 and 1-4 pair sets, the rigid
+ * fragments of the torsion tree and the scored intra pair lists, on `nthreads` host
+ * threads (0 = all cores).  The result is a ligand set in exactly the packed layout of
+ * ud_add_ligands (plus ff types, charges and the pair-set sizes), in document order.
+ * Replaces: the json.dumps + rapidjson hand-off and RapidJsonParser::parse_ligands_info
+ * with split_torsions_into_frags (api/python/pipeline.cpp:125-139,
+ * src/format/rapidjson_parser.cpp:54-225,227-296).
+ * Errors (malformed document or schema) return UD_EINVAL; the message is in
+ * ud_ligset_last_error(). */
+typedef struct ud_ligset ud_ligset;
+int ud_ligset_parse_json(const char* json, size_t len, int use_tor_lib, int nthreads, ud_ligset** out);
+/* out8 = [ligands, atoms, torsions, ranges, rotated atoms, pair entries, bias records,
+ * bytes of all names]: the lengths of the export arrays (offset arrays have one more). */
+int ud_ligset_sizes(const ud_ligset* set, long long* out8);
+/* Copy the set out; any pointer may be NULL to skip that array.  name_off[ligands+1]
+ * indexes `names` (UTF-8, not NUL-terminated). */
+int ud_ligset_export(const ud_ligset* set, int* atom_off, float* xyz, int* types, int* ff_types, float* charges,
+                     int* tors_off, int* axis, float* dihedrals, int* range_off, float* ranges, int* rot_off,
+                     int* rot_atoms, int* pair_off, int* pairs, int* bias_off, float* bias, int* n_pairs_1213,
+                     int* n_pairs_14, long long* name_off, char* names);
+void ud_ligset_free(ud_ligset* set);
+const char* ud_ligset_last_error(void);
 
 /* Drop all ligands and search results. */
 int ud_clear_ligands(ud_ctx* ctx);

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "ud2b200", "libudock_b200.so")
-SOURCES = ["ud_engine.cu"]
+SOURCES = ["ud_engine.cu", "ud_topology.cpp"]
 DEPS = SOURCES + ["ud_device.cuh", "ud_mlp.cuh", "ud_mlp_host.cuh"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]

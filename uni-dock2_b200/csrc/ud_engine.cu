@@ -1275,6 +1275,24 @@ int ud_version(void) { return 100; }
 
 const char* ud_last_error(void) { return g_err.c_str(); }
 
+int ud_device_memory(int device, long long* out_free, long long* out_total) {
+    try {
+        if (!out_free || !out_total) throw Fail(UD_EINVAL, "null argument");
+        int cur = 0;
+        ck(cudaGetDevice(&cur), "cudaGetDevice");
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        size_t fr = 0, tot = 0;
+        const cudaError_t e = cudaMemGetInfo(&fr, &tot);
+        cudaSetDevice(cur);
+        ck(e, "cudaMemGetInfo");
+        *out_free = (long long)fr;
+        *out_total = (long long)tot;
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
 int ud_create(int device, const float* box6, ud_ctx** out) {
     try {
         if (!out || !box6) throw Fail(UD_EINVAL, "null argument");

@@ -93,6 +93,12 @@ def load_library() -> C.CDLL:
         "ud_get_moves": ([vp, i, fp, fp, fp], i),
         "ud_dock_learned": ([vp, vp, f, C.POINTER(C.c_longlong)], i),
         "ud_mlp_train_moves": ([vp, i, i, f, C.c_uint64, fp], i),
+        "ud_device_memory": ([i, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], i),
+        "ud_ligset_parse_json": ([C.c_char_p, C.c_size_t, i, i, C.POINTER(C.c_void_p)], i),
+        "ud_ligset_sizes": ([vp, vp], i),
+        "ud_ligset_export": ([vp] + [vp] * 19, i),
+        "ud_ligset_free": ([vp], None),
+        "ud_ligset_last_error": ([], C.c_char_p),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -198,6 +204,7 @@ class Engine:
         b6 = box.as6()
         self._check(self.L.ud_create(device, _p(b6), C.byref(h)))
         self.h = h
+        self.device = int(device)
         self.ligands: List[Ligand] = []
         self.nchain = 0
         self.retain = 1
@@ -247,15 +254,28 @@ class Engine:
         self._check(self.L.ud_get_grid(self.h, _p(out), _p(gd), _p(org)))
         return out, gd, org
 
-    def add_ligands(self, ligs: Sequence[Ligand]):
-        if not ligs:
+    def add_ligands(self, ligs):
+        """Append ligands: a sequence of Ligand, or a LigandSet from the native bulk
+        parser (its packed arrays go to the engine as they are)."""
+        if len(ligs) == 0:
             return
-        p = pack_ligands(ligs)
+        from .ligset import LigandSet, LigandRef
+        bulk = isinstance(ligs, LigandSet)
+        p = ligs.packed() if bulk else pack_ligands(ligs)
         self._check(self.L.ud_add_ligands(self.h, len(ligs), _p(p["atom_off"]), _p(p["xyz"]), _p(p["types"]),
                                           _p(p["tors_off"]), _p(p["axis"]), _p(p["dihedrals"]), _p(p["range_off"]),
                                           _p(p["ranges"]), _p(p["rot_off"]), _p(p["rot"]), _p(p["pair_off"]),
                                           _p(p["pairs"]), _p(p["bias_off"]), _p(p["bias"])))
-        self.ligands.extend(ligs)
+        if bulk:
+            self.ligands.extend(LigandRef(ligs, i) for i in range(len(ligs)))
+        else:
+            self.ligands.extend(ligs)
+
+    def device_memory(self):
+        """(free, total) bytes of this context's device."""
+        fr, tot = C.c_longlong(0), C.c_longlong(0)
+        self._check(self.L.ud_device_memory(self.device, C.byref(fr), C.byref(tot)))
+        return int(fr.value), int(tot.value)
 
     def clear_ligands(self):
         self._check(self.L.ud_clear_ligands(self.h))

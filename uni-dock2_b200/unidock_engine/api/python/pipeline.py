@@ -8,10 +8,16 @@ engine (libudock_b200.so) instead of the reference's CUDA engine:
 * presets: search_mode fast/balance/detail/free (src/screening/core.cpp:65-84), task
   screen/score/mc/randomize/optimize (core.cpp:165-212), bias no/pos/align (core.cpp:86-97),
   constraint docking disables randomisation (core.cpp:142-146);
-* ligands are processed in the reference's size groups and batches of at most 1000
+* ligands are parsed, and their pair lists built, in bulk by the native parser
+  (``ud_ligset_parse_json``; rapidjson_parser.cpp:54-296);
+* ligands are ordered in the reference's size groups and batches of at most 1000
   (src/screening/screening.cpp:17-41,162-216), one output file per batch
   ``<output_dir>/<name_json>_<batch>.json``; ``opt_steps=-1`` resolves to
   ``(25 + max atoms of the first batch) / 3`` and keeps that value (screening.cpp:206-208);
+  the engine docks as many consecutive batches of one size group in one launch as fit the
+  device memory budget (95 % of the free memory, capped by ``max_gpu_mem`` MB;
+  core.cpp:32-63), so a ligand's chains get their random streams from its place in the
+  launch;
 * output JSON ``{ligand: [{"energy": [affinity, total, intra, inter, penalty, conf_indep,
   bias], "coords": [...], "dihedrals": [deg...], ("decomp": [[5]...])}]}``, 3 decimals,
   non-finite values clamped to +-1e6 (src/format/json.cpp:88-191, src/task/DockTask.cpp:224-282);
@@ -36,9 +42,10 @@ from typing import Dict, List, Optional
 
 import numpy as np
 
-from ud2b200.batching import batches
+from ud2b200.batching import memory_budget, plan_launches, predict_dock_bytes, reference_batches
 from ud2b200.engine import Engine, EngineError, MODE_DIRECT, MODE_GRID, GRID_F16, GRID_F32
-from ud2b200.model import Box, F32, RAD2DEG_F, parse_ligands, parse_receptor
+from ud2b200.ligset import LigandRef, parse_ligands_bulk
+from ud2b200.model import Box, F32, RAD2DEG_F, parse_receptor
 
 log = logging.getLogger("unidock_engine")
 
@@ -81,6 +88,13 @@ def _fmt_array(vals) -> List[str]:
     s = np.strings.add(np.strings.add(np.where(np.signbit(v), "-", ""), (q // 1000).astype(str)),
                        _FRAC_NP[q % 1000])
     return s.tolist()
+
+
+def _host_memory() -> int:
+    try:
+        return os.sysconf("SC_PHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except (ValueError, OSError):
+        return 0
 
 
 class DockingPipeline:
@@ -196,10 +210,11 @@ class DockingPipeline:
             log.warning("benchmark task is not implemented")
             return
         rec = parse_receptor(self._receptor, self.box)
-        ligs = parse_ligands(self._ligands, self.use_tor_lib)
-        if not ligs:
+        # all ligands parsed and their pair lists built natively, in document order
+        ls = parse_ligands_bulk(self._ligands, self.use_tor_lib)
+        if len(ls) == 0:
             log.error("No flexible molecules are found")
-        plan = batches([l.natom for l in ligs], [l.ntors for l in ligs])
+        ref_batches = reference_batches(ls.natoms, ls.ntors)
         eng = Engine(self.box, device=self.gpu_device_id)
         try:
             eng.set_flags(self.constraint_docking, p["bias_type"], self.bias_k)
@@ -210,7 +225,7 @@ class DockingPipeline:
                 eng.set_autotune(True)
             mode = MODE_GRID if self.scoring == "grid" else MODE_DIRECT
             if mode == MODE_GRID:
-                mt = sorted(set(int(t) for l in ligs for t in l.types if t != 0))
+                mt = sorted(int(t) for t in np.unique(ls.a["types"]) if t != 0)
                 if mt:
                     eng.build_grid(self.grid_spacing, mt, GRID_F16 if self.grid_precision == "f16" else GRID_F32)
                 else:
@@ -220,26 +235,48 @@ class DockingPipeline:
                 eng.mlp_set_params(self.proposal_params)
                 learned = self.p_learned
             opt_steps = p["opt_steps"]
-            batch_id = 0
+            if opt_steps == -1 and ref_batches:       # the first batch decides (screening.cpp:206-208)
+                opt_steps = (25 + int(max(ls.natoms[i] for i in ref_batches[0][1]))) // 3
+            # launches: as many of the reference's batches of one size group as fit the device
+            # memory budget (max_gpu_mem caps it); output files still one per reference batch
+            a = ls.a
+            per_lig = predict_dock_bytes(ls.natoms, ls.ntors, np.diff(a["pair_off"][a["atom_off"]]),
+                                         np.diff(a["rot_off"][a["tors_off"]]), np.diff(a["range_off"][a["tors_off"]]),
+                                         np.diff(a["bias_off"][a["atom_off"]]), nchain=p["exhaustiveness"],
+                                         retain=self.poses_per_chain, num_pose=p["num_pose"],
+                                         learned=learned is not None, decomp=self.energy_decomp)
+            free, _ = eng.device_memory()
+            budget = memory_budget(free, self.max_gpu_mem, _host_memory())
+            plan = plan_launches(ref_batches, per_lig, budget)
+            batch_of = np.empty(len(ls), np.int64)
+            left = []
+            for k, (_, b) in enumerate(ref_batches):
+                batch_of[b] = k
+                left.append(len(b))
+            done: Dict[int, object] = {}
             nevals = 0
-            for batch in plan:
-                batch_id += 1
-                bl = [ligs[i] for i in batch]
-                if opt_steps == -1:
-                    opt_steps = (25 + max(l.natom for l in bl)) // 3
+            for run in plan:
                 eng.clear_ligands()
-                eng.add_ligands(bl)
+                eng.add_ligands(ls.subset(run))
                 res, ne = eng.dock(seed=p["seed"], nchain=p["exhaustiveness"], mc_steps=p["mc_steps"],
                                    opt_steps=opt_steps, refine_steps=p["refine_steps"], num_pose=p["num_pose"],
                                    rmsd_limit=p["rmsd_limit"], energy_range=p["energy_range"],
                                    randomize=p["randomize"], mode=mode, final_mode=MODE_DIRECT,
                                    energy_decomp=self.energy_decomp, p_learned=learned)
                 nevals += ne
-                fp = os.path.join(self.output_dir, f"{self.name_json}_{batch_id}.json")
-                self._dump(fp, bl, res)
+                for i, r in zip(run, res):
+                    done[i] = r
+                    k = int(batch_of[i])
+                    left[k] -= 1
+                    if left[k] == 0:                  # a reference batch is complete: its file
+                        b = ref_batches[k][1]
+                        fp = os.path.join(self.output_dir, f"{self.name_json}_{k + 1}.json")
+                        self._dump(fp, [LigandRef(ls, j) for j in b], [done.pop(j) for j in b])
+            self.last_launches = len(plan)
         finally:
             eng.close()
-        self.last_stats = dict(seconds=time.perf_counter() - t0, evaluations=float(nevals), ligands=float(len(ligs)))
+        self.last_stats = dict(seconds=time.perf_counter() - t0, evaluations=float(nevals), ligands=float(len(ls)),
+                               launches=float(len(plan)))
 
     # ------------------------------------------------------------------ output
     def _dump(self, fp: str, ligs, results) -> None:
