@@ -164,6 +164,18 @@ int ud_score_batch(ud_ctx* ctx, int n, const int* pose_lig, const float* coords,
 int ud_score_batch_noalloc(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, const float* centers,
                            const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g);
 
+/* Measurement helpers (used by bench.py for the roofline; not part of the reference path).
+ * ud_read_bandwidth: streaming 16-byte reads of a `bytes` buffer, `repeats` times after 3
+ * warm-up passes, timed with CUDA events: the L2 read bandwidth when the buffer fits the
+ * L2 (126 MB on B200), the HBM read bandwidth when it is far larger.
+ * ud_score_batch_timed: ud_score_batch with the inputs uploaded once and the scoring
+ * kernel launched `repeats` times back to back (after one warm-up launch); out_ms is the
+ * mean kernel time.  Results as ud_score_batch.  No counterpart in the reference. */
+int ud_read_bandwidth(int device, long long bytes, int repeats, float* out_gbps);
+int ud_score_batch_timed(ud_ctx* ctx, int n, const int* pose_lig, const float* coords, const float* centers,
+                         const float* rotvecs, int mode, float vcap, float slope, int repeats, float* out_e,
+                         float* out_g, float* out_ms);
+
 /* Final-score terms of n poses without curl: out_terms4 = [intra(i<j), inter, penalty, bias]
  * per pose; out_decomp (nullable) = 5 inter terms per atom
  * [gauss1, gauss2, repulsion, hydrophobic, hbond].

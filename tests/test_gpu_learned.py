@@ -175,7 +175,8 @@ def test_untrained_learned_search_keeps_every_pose_finite(search_sys, p_learned)
     """An untrained network proposes large, arbitrary moves; the poses they lead to (some
     far outside the box, where the penalty gradient drives BFGS steps that overflow) must
     never reach a chain record or a docked pose: every record and every output pose has
-    finite energy, centre and coordinates."""
+    finite energy, centre and coordinates.  (A chain's best may still be a pose partly
+    outside the box after 12 steps, with a large finite penalty: 1e6 per A per atom.)"""
     eng = search_sys["eng"]
     ligs = search_sys["ligs"]
     eng.mlp_init(17)
@@ -183,7 +184,7 @@ def test_untrained_learned_search_keeps_every_pose_finite(search_sys, p_learned)
         eng.search_learned(seed=seed, nchain=32, mc_steps=12, opt_steps=5, p_learned=p_learned)
         for li, lig in enumerate(ligs):
             recs = eng.chain_poses(li)
-            assert np.all(np.isfinite(recs[:, 0])) and np.all(recs[:, 0] < 1e8), (seed, li)
+            assert np.all(np.isfinite(recs[:, 0])) and np.all(recs[:, 0] < 1e9), (seed, li)
             assert np.all(np.isfinite(recs[:, 1:4])), (seed, li)
             assert np.all(np.isfinite(recs[:, 8:8 + 3 * lig.natom + lig.ntors])), (seed, li)
     res, _ = eng.dock(seed=43, nchain=16, mc_steps=8, opt_steps=4, refine_steps=2, num_pose=3, rmsd_limit=1.0,

@@ -64,16 +64,16 @@ def test_pipeline_with_learned_proposal_and_kept_poses(tmp_path, small_system):
 
 
 def test_pipeline_launches_follow_the_memory_budget(tmp_path, small_system):
-    """All ligands of the small system share one size group: with the default budget they
-    dock in one launch; with max_gpu_mem just above the largest ligand's predicted bytes
-    (4096 chains) they dock in the launches the plan gives for that budget.  The output
-    files and their layout are the same either way."""
-    from ud2b200.batching import plan_launches, predict_dock_bytes, reference_batches
+    """With the default budget the ligands dock in one launch per size group (the small
+    system's 41-atom ligand is in the second group); with max_gpu_mem just above the
+    largest ligand's predicted bytes (4096 chains) they dock in the launches the plan gives
+    for that budget.  The output files and their layout are the same either way."""
+    from ud2b200.batching import plan_launches, predict_dock_bytes, reference_batches, size_groups
     from ud2b200.ligset import parse_ligands_bulk
     kw = dict(exhaustiveness=4096, mc_steps=2)
-    p1, out1 = _run(tmp_path / "one", small_system, **kw)
-    assert p1.last_stats["launches"] == 1
     ls = parse_ligands_bulk(small_system["ligd"])
+    p1, out1 = _run(tmp_path / "one", small_system, **kw)
+    assert p1.last_stats["launches"] == sum(1 for g in size_groups(ls.natoms, ls.ntors) if g) == 2
     a = ls.a
     per = predict_dock_bytes(ls.natoms, ls.ntors, np.diff(a["pair_off"][a["atom_off"]]),
                              np.diff(a["rot_off"][a["tors_off"]]), np.diff(a["range_off"][a["tors_off"]]),

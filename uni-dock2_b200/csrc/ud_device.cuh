@@ -255,6 +255,65 @@ __device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
 // ---------------------------------------------------------------- warp helpers
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
+// ---------------------------------------------------------------- topology staging (TMA)
+// A work item's topology blob goes from global to the CTA's shared memory as one bulk
+// asynchronous copy on the tensor-memory-access engine (cp.async.bulk, no multicast),
+// completing on an mbarrier.  Both addresses are 16-byte aligned and the size is a multiple
+// of 16 bytes (blobs are padded to 4 words and start at 4-word offsets); every thread waits
+// on the barrier's phase with a bounded spin.
+constexpr long long STAGE_SPIN = 1LL << 24;
+
+__device__ __forceinline__ uint32_t cta_smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void stage_bar_init(uint64_t* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(cta_smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// one thread: arm the barrier for `bytes` and start the copy
+__device__ __forceinline__ void stage_bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(cta_smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(cta_smem_addr(dst)), "l"(src), "r"(bytes), "r"(cta_smem_addr(bar)) : "memory");
+}
+
+// every thread: wait for the phase with parity `parity`; false after STAGE_SPIN polls
+__device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity) {
+    for (long long i = 0; i < STAGE_SPIN; i++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done) : "r"(cta_smem_addr(bar)), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Stage `words` ints of a blob into sblob: by bulk copy when both ends are 16-byte aligned
+// and the size a multiple of 16 bytes, else by the CTA's threads.  Call from every thread
+// after a __syncthreads; returns false (in every thread) when the copy did not complete.
+__device__ __forceinline__ bool stage_blob(int* sblob, const int* src, int words, uint64_t* bar, uint32_t& phase,
+                                           int* s_flag) {
+    const bool bulk = ((reinterpret_cast<uintptr_t>(src) | cta_smem_addr(sblob)) & 15u) == 0 && (words & 3) == 0;
+    if (!bulk) {
+        for (int w = threadIdx.x; w < words; w += blockDim.x) sblob[w] = src[w];
+        return true;
+    }
+    if (threadIdx.x == 0) {
+        *s_flag = 0;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        stage_bulk_copy(sblob, src, (uint32_t)words * 4u, bar);
+    }
+    __syncthreads();
+    if (!stage_wait(bar, phase & 1u)) atomicOr(s_flag, 1);
+    phase++;
+    __syncthreads();
+    return *s_flag == 0;
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);

@@ -189,6 +189,21 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
     for (int i = lane; i < 6 + T.ntors; i += WARP) g[i] = W.g[i];
 }
 
+// ---------------------------------------------------------------------- bandwidth probe
+// Streaming read of a buffer (16-byte loads, grid-stride), summed so the loads are kept;
+// one partial sum per thread block.  With a buffer that fits the L2 the repeated reads are
+// L2 hits (the L2 read bandwidth); with one far larger, HBM reads.
+__global__ void __launch_bounds__(512) k_read_probe(const float4* __restrict__ buf, long long n4, float* out) {
+    float s = 0.f;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+        const float4 v = __ldcg(buf + i);
+        s += (v.x + v.y) + (v.z + v.w);
+    }
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out + blockIdx.x, s);
+}
+
 // ---------------------------------------------------------------------- no-allocation scoring
 // Staging area of ud_score_batch_noalloc: one per device (module-scope, allocated when the
 // module loads), shared by every context on that device.  Holds, 256-byte aligned in
@@ -456,9 +471,18 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
     bool learned = false;
     if (prop.out) learned = u01(rng.draw((uint32_t)step, P_LEARN).x) < prop.p_learned;
     if (learned) {
-        // sample m ~ N(mean, exp(logvar)) per dimension (Box-Muller on Philox draws), clamp
-        // the rigid part to a sane step, apply as one update of the candidate
+        // One degree of freedom moves, chosen as the random move chooses it (mc.cu:158-169):
+        // the centre, the orientation or one torsion.  Its change is a sample of the
+        // network's Gaussian for those dimensions, m ~ N(mean, exp(logvar)) (Box-Muller on
+        // Philox draws), in place of the random move's uniform draw; the rigid part is
+        // clamped to a step of the random move's size.  Applied as one update of the
+        // candidate.
         const int dim = 6 + T.ntors;
+        const int nmut = 2 + T.ntors;
+        const uint32_t uw = rng.draw((uint32_t)step, P_WHICH).x;
+        const int which = env.constraint ? (nmut < 3 ? 3 : 2 + (int)(uw % (uint32_t)(nmut - 2)))
+                                         : (int)(uw % (uint32_t)nmut);
+        const bool mine = which == 0 ? lane < 3 : (which == 1 ? (lane >= 3 && lane < 6) : lane == 4 + which);
         if (lane < dim) {
             const U4 u = rng.draw((uint32_t)step, P_LNORM + (lane >> 2));
             const uint32_t ua = (lane & 2) ? u.z : u.x, ub = (lane & 2) ? u.w : u.y;
@@ -468,10 +492,10 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
             const float z = (lane & 1) ? r * sn : r * cs;
             const float lv = fminf(fmaxf(prop.out[26 + lane], -8.f), 4.f);
             float m = prop.out[lane] + __expf(0.5f * lv) * z;
-            if (lane < 3) m = fminf(fmaxf(m, -4.f), 4.f);
+            if (lane < 3) m = fminf(fmaxf(m, -2.f), 2.f);
             else if (lane < 6) m = fminf(fmaxf(m, -PI_F), PI_F);
             else m = fminf(fmaxf(m, -2.f * PI_F), 2.f * PI_F);
-            if (lane < 6 && env.constraint) m = 0.f;
+            if ((lane < 6 && env.constraint) || !mine) m = 0.f;
             if (!(m == m)) m = 0.f;
             W.p[lane] = m;
         }
@@ -537,7 +561,10 @@ __global__ void __launch_bounds__(NT, MINB) k_search(const int* __restrict__ blo
     const int warp = threadIdx.x >> 5, lane = lane_id();
     float* ws = wsbase + (size_t)warp * sp.ws_max;
     unsigned long long my_evals = 0, my_heavy = 0;
-    if (threadIdx.x == 0) s_lig = -1;
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_flag;
+    uint32_t phase = 0;
+    if (threadIdx.x == 0) { s_lig = -1; stage_bar_init(&s_bar); }
     while (true) {
         if (threadIdx.x == 0) { s_item = atomicAdd(work_counter, 1); s_next = 0; }
         __syncthreads();
@@ -545,8 +572,9 @@ __global__ void __launch_bounds__(NT, MINB) k_search(const int* __restrict__ blo
         if (it >= nitems) break;
         const int4 item = items[it];          // (ligand, first chain, count, -)
         const LigDev L = ligs[item.x];
-        if (item.x != s_lig) {
-            for (int w = threadIdx.x; w < L.stage_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+        if (item.x != s_lig && !stage_blob(sblob, blobs + L.blob_off, L.stage_words, &s_bar, phase, &s_flag)) {
+            if (threadIdx.x == 0 && nevals) atomicAdd(nevals + 2, 1ull);
+            break;
         }
         __syncthreads();
         if (threadIdx.x == 0) s_lig = item.x;
@@ -901,7 +929,10 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
     float* ws = wsbase + (size_t)warp * sp.ws_max;
     const int step = *step_p;
     unsigned long long my_evals = 0, my_heavy = 0;
-    if (threadIdx.x == 0) s_lig = -1;
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ int s_flag;
+    uint32_t phase = 0;
+    if (threadIdx.x == 0) { s_lig = -1; stage_bar_init(&s_bar); }
     while (true) {
         if (threadIdx.x == 0) { s_item = atomicAdd(work_counter, 1); s_next = 0; }
         __syncthreads();
@@ -909,8 +940,10 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
         if (it >= nitems) break;
         const int4 item = items[it];
         const LigDev L = ligs[item.x];
-        if (item.x != s_lig)
-            for (int w = threadIdx.x; w < L.stage_words; w += blockDim.x) sblob[w] = blobs[L.blob_off + w];
+        if (item.x != s_lig && !stage_blob(sblob, blobs + L.blob_off, L.stage_words, &s_bar, phase, &s_flag)) {
+            if (threadIdx.x == 0 && nevals) atomicAdd(nevals + 2, 1ull);
+            break;
+        }
         __syncthreads();
         if (threadIdx.x == 0) s_lig = item.x;
         const Topo T = topo_view(sblob);
@@ -1720,6 +1753,103 @@ int ud_score_batch(ud_ctx* c, int n, const int* pose_lig, const float* coords, c
     }
 }
 
+int ud_read_bandwidth(int device, long long bytes, int repeats, float* out_gbps) {
+    try {
+        if (bytes < (1 << 20) || repeats < 1 || !out_gbps) throw Fail(UD_EINVAL, "invalid probe arguments");
+        ck(cudaSetDevice(device), "cudaSetDevice");
+        int nsm = 0;
+        ck(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device), "attribute");
+        const long long n4 = bytes / 16;
+        const int grid = nsm * 4;
+        DBuf<float4> buf;
+        DBuf<float> part;
+        buf.ensure((size_t)n4);
+        part.ensure((size_t)grid);
+        cudaStream_t st;
+        ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream");
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        ck(cudaMemsetAsync(buf.p, 0, (size_t)n4 * 16, st), "memset");
+        ck(cudaMemsetAsync(part.p, 0, (size_t)grid * 4, st), "memset");
+        for (int w = 0; w < 3; w++) k_read_probe<<<grid, 512, 0, st>>>(buf.p, n4, part.p);
+        ck(cudaEventRecord(e0, st), "event");
+        for (int r = 0; r < repeats; r++) k_read_probe<<<grid, 512, 0, st>>>(buf.p, n4, part.p);
+        ck(cudaEventRecord(e1, st), "event");
+        ck(cudaGetLastError(), "k_read_probe launch");
+        ck(cudaEventSynchronize(e1), "probe");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(st);
+        *out_gbps = (float)((double)n4 * 16.0 * repeats / (ms * 1e-3) / 1e9);
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
+int ud_score_batch_timed(ud_ctx* c, int n, const int* pose_lig, const float* coords, const float* centers,
+                         const float* rotvecs, int mode, float vcap, float slope, int repeats, float* out_e,
+                         float* out_g, float* out_ms) {
+    try {
+        if (!c || n <= 0 || repeats < 1 || !pose_lig || !coords || !centers || !rotvecs || !out_e || !out_g || !out_ms)
+            throw Fail(UD_EINVAL, "invalid score arguments");
+        ck(cudaSetDevice(c->device), "cudaSetDevice");
+        sync_ligs(c);
+        Env env = make_env(c, mode);
+        std::vector<long long> xoff(n), goff(n);
+        long long xs = 0, gs = 0;
+        int wsm = 0;
+        for (int i = 0; i < n; i++) {
+            int l = pose_lig[i];
+            if (l < 0 || l >= (int)c->h_ligs.size()) throw Fail(UD_EINVAL, "pose ligand index out of range");
+            xoff[i] = xs;
+            goff[i] = gs;
+            xs += 3LL * c->h_ligs[l].natom;
+            gs += 6 + c->h_ligs[l].ntors;
+            wsm = std::max(wsm, lig_ws(c->h_ligs[l]));
+        }
+        DBuf<int> dl; DBuf<long long> dxo, dgo; DBuf<float> dx, dc, dr, de, dg;
+        dl.upload(pose_lig, n, c->stream);
+        dxo.upload(xoff.data(), n, c->stream);
+        dgo.upload(goff.data(), n, c->stream);
+        dx.upload(coords, xs, c->stream);
+        dc.upload(centers, 3 * (size_t)n, c->stream);
+        dr.upload(rotvecs, 3 * (size_t)n, c->stream);
+        de.ensure(n);
+        dg.ensure(gs);
+        int W = pick_warps(c, wsm, 0, 8);
+        size_t smem = (size_t)W * wsm * 4;
+        set_smem(k_score, smem);
+        PoseIO io{dl.p, dxo.p, dx.p, dc.p, dr.p, dgo.p};
+        const unsigned grid = (unsigned)((n + W - 1) / W);
+        cudaEvent_t e0, e1;
+        ck(cudaEventCreate(&e0), "event");
+        ck(cudaEventCreate(&e1), "event");
+        k_score<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, de.p, dg.p);
+        ck(cudaEventRecord(e0, c->stream), "event");
+        for (int r = 0; r < repeats; r++)
+            k_score<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, de.p,
+                                                       dg.p);
+        ck(cudaEventRecord(e1, c->stream), "event");
+        ck(cudaGetLastError(), "k_score launch");
+        ck(cudaEventSynchronize(e1), "k_score");
+        float ms = 0.f;
+        ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *out_ms = ms / repeats;
+        ck(cudaMemcpyAsync(out_e, de.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaMemcpyAsync(out_g, dg.p, gs * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
+        ck(cudaStreamSynchronize(c->stream), "k_score");
+        return UD_OK;
+    } catch (const Fail& f) {
+        return fail(f);
+    }
+}
+
 int ud_score_terms(ud_ctx* c, int n, const int* pose_lig, const float* coords, int mode, float* out4,
                    float* out_decomp) {
     try {
@@ -1895,9 +2025,9 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, K k12, int want
     P.grid = (int)std::min((long long)P.nitems, resident);
     c->shape[0] = P.W; c->shape[1] = per_sm; c->shape[2] = P.minb; c->shape[3] = k;
     c->d_counter.ensure(1);
-    c->d_nevals.ensure(2);
+    c->d_nevals.ensure(3);          // evaluations, heavy-atom evaluations, staging timeouts
     ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
-    ck(cudaMemsetAsync(c->d_nevals.p, 0, 2 * sizeof(unsigned long long), c->stream), "memset");
+    ck(cudaMemsetAsync(c->d_nevals.p, 0, 3 * sizeof(unsigned long long), c->stream), "memset");
     c->counters[3] = total_chains;
     return P;
 }
@@ -2094,11 +2224,12 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
 }
 
 static void read_search_counters(ud_ctx* c) {
-    unsigned long long ne[2] = {0, 0};
+    unsigned long long ne[3] = {0, 0, 0};
     ck(cudaMemcpyAsync(ne, c->d_nevals.p, sizeof(ne), cudaMemcpyDeviceToHost, c->stream), "D2H");
     ck(cudaStreamSynchronize(c->stream), "search counters");
     c->counters[0] = (long long)ne[0];
     c->counters[1] = (long long)ne[1];
+    if (ne[2]) throw Fail(UD_ECUDA, "search: a topology bulk copy did not complete within its wait limit");
 }
 
 int ud_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode,

@@ -36,6 +36,15 @@ def lib_path() -> str:
     return os.environ.get("UDOCK_B200_LIB") or os.path.join(HERE, LIB_NAME)
 
 
+def read_bandwidth(device: int, nbytes: int, repeats: int = 20) -> float:
+    """GB/s of streaming reads of an nbytes buffer on `device` (L2 when it fits, else HBM)."""
+    L = load_library()
+    out = C.c_float(0.0)
+    if L.ud_read_bandwidth(int(device), int(nbytes), int(repeats), C.byref(out)) != 0:
+        raise EngineError(L.ud_last_error().decode(errors="replace"))
+    return float(out.value)
+
+
 def load_library() -> C.CDLL:
     """Load the CUDA engine; raises EngineError when it has not been built."""
     global _lib
@@ -93,6 +102,8 @@ def load_library() -> C.CDLL:
         "ud_get_moves": ([vp, i, fp, fp, fp], i),
         "ud_dock_learned": ([vp, vp, f, C.POINTER(C.c_longlong)], i),
         "ud_mlp_train_moves": ([vp, i, i, f, C.c_uint64, fp], i),
+        "ud_read_bandwidth": ([i, C.c_longlong, i, fp], i),
+        "ud_score_batch_timed": ([vp, i, ip, fp, fp, fp, i, f, f, i, fp, fp, fp], i),
         "ud_device_memory": ([i, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], i),
         "ud_ligset_parse_json": ([C.c_char_p, C.c_size_t, i, i, C.POINTER(C.c_void_p)], i),
         "ud_ligset_sizes": ([vp, vp], i),
@@ -295,6 +306,22 @@ class Engine:
                                           float(slope), _p(e), _p(g)))
         gs = np.split(g, np.cumsum(dims)[:-1]) if len(dims) > 1 else [g]
         return e, gs
+
+    def score_batch_timed(self, pose_lig: Sequence[int], coords: Sequence[np.ndarray], centers, rotvecs,
+                          mode: int = MODE_GRID, vcap: float = 1e30, slope: float = 1e6, repeats: int = 5):
+        """score_batch with the inputs resident on the device: (energies, gradients, mean
+        kernel ms over `repeats` launches)."""
+        pl = np.ascontiguousarray(pose_lig, np.int32)
+        x = np.ascontiguousarray(np.concatenate([np.asarray(c, np.float32).reshape(-1) for c in coords]))
+        ce = np.ascontiguousarray(centers, np.float32).reshape(-1)
+        rv = np.ascontiguousarray(rotvecs, np.float32).reshape(-1)
+        dims = np.array([6 + self.ligands[l].ntors for l in range(len(self.ligands))], np.int64)[pl]
+        e = np.zeros(len(pl), np.float32)
+        g = np.zeros(int(dims.sum()), np.float32)
+        ms = C.c_float(0.0)
+        self._check(self.L.ud_score_batch_timed(self.h, len(pl), _p(pl), _p(x), _p(ce), _p(rv), int(mode),
+                                                float(vcap), float(slope), int(repeats), _p(e), _p(g), C.byref(ms)))
+        return e, g, float(ms.value)
 
     def score_batch_noalloc(self, pose_lig: Sequence[int], coords: Sequence[np.ndarray], centers, rotvecs,
                             mode: int = MODE_GRID, vcap: float = 1e30, slope: float = 1e6):
