@@ -8,14 +8,27 @@ Poisson(5) rotatable bonds (clipped 0-12), a 30 A box with 0.375 A grid maps (81
 rounds of the cluster leaders, top-9 poses at RMSD 1.0 A, final scoring.  A step docks one
 batch of ligands completely.  Inputs are seeded synthetic data.
 
-Default (--mode learned): the plain fused engine docks the batch once at 4000 MC steps (the
-reference result and the plain throughput); a proposal network is trained on the GPU from
-the plain engine's searches of four other seeded ligand sets; the timed steps dock the batch
-with the learned-proposal engine at --learned-steps MC steps.  `value` is the learned
-engine's ligands/s, `quality` the share of ligands whose best score is within 0.3 kcal/mol of
-the 4000-step result.  --mode plain times the fused 4000-step engine instead.
+Default (--mode learned):
+* fresh ligands: the timed steps cycle through P = min(steps, --pool) batches of --ligands
+  ligands, each from its own seed (step k docks batch k mod P), none shared with the
+  training sets or the warm-up batch; every batch's gate reference is the plain fused
+  engine at the workload's 4000 MC steps (also reported as the plain throughput, with its
+  end-to-end rate);
+* a proposal network is trained on the GPU from the plain engine's searches of four other
+  seeded ligand sets;
+* a step sweep of both engines on batch 0 (--sweep) gives each engine's gate step count, the
+  smallest S with >= 95 % of ligands within 0.3 kcal/mol of the reference;
+* the timed steps dock with the learned engine at its gate step count (`value`, device
+  time; `e2e` through the public API with host buffers); the plain engine at its own gate
+  step count on the same batches is `plain_at_gate`, and `learned_vs_plain_at_gate` their
+  ratio;
+* also: the measured L2 and HBM read peaks, a standalone roofline of the scoring kernel on
+  ~1e6 resident poses, a 65,536-ligand uneven launch (config 2 scale), the reference's own
+  CUDA engine on a small batch when oracle/_ref/udref_dock is built, and the CPU baseline.
+--mode plain times the fused 4000-step engine instead.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--mode learned|plain]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
+                    [--mode learned|plain]
 
 N > 1 runs under torchrun, one rank per GPU, each rank docking its own ligands (weak
 scaling, no data-path collective); the timed region is bracketed by a barrier and
@@ -34,10 +47,34 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "uni-dock2_b200"))
 
 METRIC = "ligands/s @ best-score within 0.3 kcal/mol of ref; learned vs plain search"
+T_START = time.perf_counter()
+
+
+def log(msg: str) -> None:
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - T_START:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
+def _jsonable(o):
+    if isinstance(o, np.integer):
+        return int(o)
+    if isinstance(o, np.floating):
+        return float(o)
+    if isinstance(o, np.bool_):
+        return bool(o)
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError(f"not JSON serialisable: {type(o).__name__}")
+
+
+def emit_line(out: dict) -> None:
+    print(json.dumps(out, default=_jsonable), flush=True)
 UNIT = "ligands/s"
 
 
@@ -48,7 +85,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--ref-ligands", type=int, default=8, help="ligands of the reference-gpu comparison")
-    ap.add_argument("--ref-mc-steps", type=int, default=200, help="MC steps of the reference-gpu comparison")
+    ap.add_argument("--ref-mc-steps", type=int, default=100, help="MC steps of the reference-gpu comparison")
     ap.add_argument("--workload", default="screen")
     ap.add_argument("--ligands", type=int, default=148, help="ligands per step per GPU")
     ap.add_argument("--mc-steps", type=int, default=0, help="override MC steps (0 = workload value)")
@@ -57,10 +94,14 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--grid", default="f32", choices=["f32", "f16"])
     ap.add_argument("--mode", default="learned", choices=["learned", "plain"])
-    ap.add_argument("--learned-steps", type=int, default=1000, help="MC steps of the learned-proposal engine")
+    ap.add_argument("--learned-steps", type=int, default=400,
+                    help="MC steps of the timed learned-proposal engine (the step sweep's gate count on the screen batch)")
     ap.add_argument("--p-learned", type=float, default=0.25, help="share of learned moves")
     ap.add_argument("--train-ligands", type=int, default=37, help="training ligands per seed (4 seeds)")
     ap.add_argument("--train-epochs", type=int, default=6, help="epochs of network training")
+    ap.add_argument("--pool", type=int, default=3, help="fresh ligand batches the timed steps cycle through")
+    ap.add_argument("--sweep", default="50,100,200,400,1000", help="MC steps of the step sweep")
+    ap.add_argument("--no-extras", action="store_true", help="skip the 65,536-ligand and reference-engine blocks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     return ap.parse_args()
@@ -237,35 +278,45 @@ def reference_scoring_rate(rec, box, ligs, seconds: float = 8.0):
 # ------------------------------------------------------------------------- main arms
 def run_reference(a):
     """The reference's CPU path on this host: the oracle restatement of the reference's
-    search (direct-sum scoring as the reference), timed on bounded samples."""
-    import numpy as np
+    search (MC chains with BFGS, direct-sum scoring as the reference) on all host cores,
+    each step a bounded sample of the same workload as this engine's arm: the same fresh
+    ligand batch 0, chains, MC steps and opt_steps.  The search is > 95 % of a dock's work;
+    clustering, refinement and final scoring are not sampled."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from ud2b200.batching import heuristic_opt_steps
-    nl = max(8, os.cpu_count() or 8)
-    w, box, rec, ligs = make_inputs(a.workload, nl, a.seed, 0)
-    mc = a.mc_steps or w["mc_steps"]
-    opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
+    w, box, rec, _ = make_inputs(a.workload, 1, a.seed, 0)
+    center = (box.lo.astype(np.float64) + box.hi) / 2.0
+    from ud2b200 import synth
+    core = synth.make_core(center, a.seed) if a.workload == "template" else None
+    batch0 = ligand_batch(a.workload, a.ligands, a.seed * 1000 + 11, 0, center, core)
+    mc = arm_mc_steps(a, w)
+    opt = heuristic_opt_steps([l.natom for l in batch0], [l.ntors for l in batch0])
+    P = max(1, min(a.steps, a.pool))
     per_step = max(2.0, min(30.0, 120.0 / max(1, a.steps + a.warmup)))
-    rates = []
-    for s in range(a.warmup + a.steps):
-        r, cores, sample = cpu_port_rate(w, box, rec, ligs, mc, opt, per_step)
-        if s >= a.warmup:
+    rates, secs = [], []
+    for st in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        r, cores, sample = cpu_port_rate(w, box, rec, batch0, mc, opt, per_step)
+        if st >= a.warmup:
             rates.append(r)
+            secs.append(time.perf_counter() - t0)
     rate = statistics.mean(rates)
     lig_s = rate / (w["chains"] * mc)
     out = {"metric": METRIC, "value": lig_s, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-           "ms_per_step": 1000.0 / lig_s, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f32", "data": "synthetic", "impl": "reference",
-           "config": {"workload": a.workload, "chains": w["chains"], "mc_steps": mc, "opt_steps": opt,
-                      "receptor_atoms": rec.natom, "box_A": w["box"]},
+           "ms_per_step": 1000.0 * statistics.mean(secs), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+           "config": workload_config(a, w, rec, opt, mc, P, 1),
+           "engine_config": {"engine": "the reference's search restated on the CPU (oracle port), direct sums",
+                             "step": f"a bounded sample: {per_step:.0f} s of MC chain steps on all host cores; "
+                                     "value = sampled chain steps/s over chains x MC steps per ligand"},
            "cpu_baseline": {"value": lig_s, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
            "e2e": {"value": lig_s, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    ref_sc = reference_scoring_rate(rec, box, ligs)
+    ref_sc = reference_scoring_rate(rec, box, batch0)
     if ref_sc:
         out["reference_cpu_scoring"] = ref_sc
-    print(json.dumps(out), flush=True)
+    emit_line(out)
 
 
 def reduce_over_ranks(dist, dev_ms: float, e2e_s: float, ligs_done: int, device: str):
@@ -296,7 +347,7 @@ def top_scores(res):
     return [float(r.terms[0].sum()) if len(r.records) else float("inf") for r in res]
 
 
-def run_reference_gpu(a):
+def run_reference_gpu(a, emit: bool = True):
     """The reference's own CUDA engine (core_pipeline, built from its sources into
     oracle/_ref/udref_dock) and this engine on the same small batch and settings, both on
     this GPU; ligands/s are extrapolated to the workload's MC steps (the time is linear in
@@ -308,8 +359,10 @@ def run_reference_gpu(a):
     from ud2b200.model import Box, parse_ligands, parse_receptor
     exe = os.path.join(ROOT, "oracle", "_ref", "udref_dock")
     if not os.path.exists(exe):
-        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/udref_dock not built (make -C oracle refengine)"}))
-        return
+        if emit:
+            print(json.dumps({"impl": "reference-gpu",
+                              "unavailable": "oracle/_ref/udref_dock not built (make -C oracle refengine)"}))
+        return None
     w = synth.WORKLOADS[a.workload]
     rows, center = synth.make_receptor(w["nrec"], w["cube"], a.seed)
     box = Box.from_center_size(center, [w["box"]] * 3)
@@ -361,14 +414,147 @@ def run_reference_gpu(a):
            "quality": quality,
            "note": "wall times of one call each on the same GPU and inputs; ligands/s extrapolated linearly "
                    f"from {steps} to {w['mc_steps']} MC steps"}
-    print(json.dumps(out), flush=True)
+    if emit:
+        emit_line(out)
+    return out
+
+
+def workload_config(a, w, rec, opt: int, mc_steps: int, P: int, world: int) -> dict:
+    """The workload an arm runs (identical in both arms; engine details are reported apart)."""
+    template = a.workload == "template"
+    return {"workload": a.workload, "ligands_per_step_per_gpu": a.ligands, "fresh_batches": P, "chains": w["chains"],
+            "mc_steps": mc_steps, "opt_steps": opt, "refine_steps": 5, "num_pose": w["num_pose"],
+            "rmsd_limit": w["rmsd"], "receptor_atoms": rec.natom, "box_A": w["box"], "grid_spacing_A": 0.375,
+            "constraint_docking": template, "poses_kept_per_chain": 4 if template else 1,
+            "batches": f"timed step k docks fresh batch k mod {P} ({a.ligands} ligands, its own seed)",
+            "l2": "flushed between steps (256 MB write)", "parallelism": f"ligand shards x{world}"}
+
+
+def arm_mc_steps(a, w) -> int:
+    """MC steps per chain of the timed steps: the learned engine's step count in learned
+    mode, else the workload's."""
+    return a.mc_steps or (a.learned_steps if a.mode == "learned" else w["mc_steps"])
+
+
+def ligand_batch(workload: str, nlig: int, lig_seed: int, rank: int, center, core=None):
+    """A batch of the workload's ligands from its own seed (the receptor is shared)."""
+    from ud2b200 import synth
+    from ud2b200.model import parse_ligands
+    sizes = synth.ligand_sizes(workload, nlig * (rank + 1), lig_seed)[nlig * rank:]
+    d = {f"s{lig_seed}_r{rank}_{i:05d}": synth.make_ligand(n, t, lig_seed * 7919 + rank * 1000003 + i, center,
+                                                            core=core)
+         for i, (n, t) in enumerate(sizes)}
+    return parse_ligands(d)
+
+
+def dock_timed(eng, ligs, kw, flush, p_learned=None):
+    """One dock through the public API: (results, device ms, wall s, counters)."""
+    import torch
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    eng.clear_ligands()
+    eng.add_ligands(ligs)
+    res, _ = eng.dock(**kw, fetch=True, p_learned=p_learned)
+    wall = time.perf_counter() - t0
+    return res, float(eng.stage_times()[5]), wall, eng.counters(), eng.stage_times().tolist()
+
+
+def random_rigid_poses(ligs, n_per, rng):
+    """n_per rigid placements of each ligand's input conformation inside the central 20 A
+    of the box: flat coordinates, centres, rotation vectors and the ligand of each pose."""
+    from scipy.spatial.transform import Rotation as Rot
+    xs, cs, rs, pl = [], [], [], []
+    for li, lig in enumerate(ligs):
+        x0 = lig.coords.astype(np.float64) - lig.coords.astype(np.float64).mean(axis=0)
+        R = Rot.random(n_per, random_state=rng).as_matrix()
+        t = lig.center.astype(np.float64) + rng.uniform(-6.0, 6.0, (n_per, 3))
+        X = np.einsum("pij,aj->pai", R, x0) + t[:, None, :]
+        xs.append(X.astype(np.float32).reshape(-1))
+        cs.append(t.astype(np.float32))
+        rs.append(rng.uniform(-1.0, 1.0, (n_per, 3)).astype(np.float32))
+        pl.append(np.full(n_per, li, np.int32))
+    return np.concatenate(xs), np.concatenate(cs), np.concatenate(rs), np.concatenate(pl)
+
+
+def kscore_roofline(eng, ligs, peaks, grid: str):
+    """The scoring kernel alone (k_score, warp per pose: grid E + force, intra pairs,
+    generalised gradient) on ~1e6 poses resident in HBM, timed over 5 launches."""
+    eng.clear_ligands()
+    eng.add_ligands(ligs)
+    rng = np.random.default_rng(11)
+    n_per = max(1, 1_000_000 // len(ligs))
+    x, c, r, pl = random_rigid_poses(ligs, n_per, rng)
+    from ud2b200 import MODE_GRID
+    e, g, ms = eng.score_batch_timed(pl, [x], c, r, mode=MODE_GRID, vcap=10.0, slope=1e6, repeats=5)
+    nat = np.array([l.natom for l in ligs])[pl]
+    nhv = np.array([l.n_heavy for l in ligs])[pl]
+    ntor = np.array([l.ntors for l in ligs])[pl]
+    s = 2 if grid == "f16" else 4
+    map_bytes = float(np.sum(nhv) * 8 * s)
+    io_bytes = float(np.sum(12 * nat + 4 + 24 + 4 + 4 * (6 + ntor) + 4 + 16))
+    t = ms * 1e-3
+    return {"kernel": "k_score", "poses": int(len(pl)), "ms_per_launch": ms, "poses_per_s": len(pl) / t,
+            "map_bytes_per_launch": map_bytes, "pose_io_bytes_per_launch": io_bytes,
+            "l2": {"achieved_gbs": (map_bytes + io_bytes) / t / 1e9, "peak_gbs": peaks["l2_gbs"],
+                   "frac": (map_bytes + io_bytes) / t / 1e9 / peaks["l2_gbs"],
+                   "note": "map reads (L2-resident maps) plus pose I/O over the measured L2 read peak"},
+            "hbm": {"achieved_gbs": io_bytes / t / 1e9, "peak_gbs": peaks["hbm_gbs"],
+                    "frac": io_bytes / t / 1e9 / peaks["hbm_gbs"],
+                    "note": "pose coordinates in, energy and gradient out, over the measured HBM copy peak"},
+            "finite": bool(np.all(np.isfinite(e)))}
+
+
+def uneven_full(a, w, box, rec, local, nlig=65536, chains=128, mc_steps=2):
+    """Config-2 scale: 65,536 uneven ligands (8-80 heavy atoms, 0-20 torsions; 512 distinct
+    topologies, each repeated under its own name, so every ligand has its own chains and
+    random streams) parsed in bulk from their JSON text and docked in one persistent launch
+    on FP16 maps; the refinement scores on the maps too (its exact-sum default takes minutes
+    at this size)."""
+    from ud2b200 import Engine, GRID_F16, MODE_GRID, synth
+    from ud2b200.batching import heuristic_opt_steps
+    from ud2b200.ligset import parse_ligands_bulk
+    center = (box.lo.astype(np.float64) + box.hi) / 2.0
+    sizes = synth.ligand_sizes("uneven", 512, a.seed + 77)
+    parts = [json.dumps(synth.make_ligand(n, t, (a.seed + 77) * 7919 + i, center)) for i, (n, t) in enumerate(sizes)]
+    text = "{" + ",".join(f'"u{i:06d}":{parts[i % len(parts)]}' for i in range(nlig)) + "}"
+    t0 = time.perf_counter()
+    ls = parse_ligands_bulk(text)
+    parse_s = time.perf_counter() - t0
+    mt = sorted(int(t) for t in np.unique(ls.a["types"]) if t != 0)
+    opt = heuristic_opt_steps(ls.natoms, ls.ntors)
+    eng = Engine(box, device=local)
+    try:
+        eng.set_receptor(rec.xyz, rec.types)
+        eng.build_grid(0.375, mt, GRID_F16)
+        t0 = time.perf_counter()
+        eng.add_ligands(ls)
+        res, ne = eng.dock(seed=a.seed, nchain=chains, mc_steps=mc_steps, opt_steps=opt, refine_steps=5, num_pose=9,
+                           rmsd_limit=1.0, energy_range=10.0, randomize=True, mode=MODE_GRID, fetch=True,
+                           refine_mode=MODE_GRID)
+        wall = time.perf_counter() - t0
+        st = eng.stage_times().tolist()
+        shape = eng.search_shape()
+        cn = eng.counters()
+    finally:
+        eng.close()
+    top = np.array(top_scores(res))
+    return {"workload": "uneven", "ligands": nlig, "distinct_topologies": 512, "chains": chains, "mc_steps": mc_steps,
+            "opt_steps": opt, "grid_precision": "f16", "json_mb": len(text) / 1e6, "bulk_parse_s": parse_s,
+            "device_ms": st[5], "stage_ms": st, "search_launches": 1, "search_shape": shape,
+            "ligands_per_s_device": nlig / (st[5] / 1000.0), "ligands_per_s_e2e": nlig / wall,
+            "evaluations": cn["evaluations"], "evaluations_per_s": cn["evaluations"] / (st[0] / 1000.0),
+            "finite_top_scores": bool(np.all(np.isfinite(top))),
+            "refine_mode": "grid",
+            "note": f"one k_search launch over {nlig} ligands x {chains} chains at {mc_steps} MC steps (a scale run, "
+                    "not a quality run); e2e includes ligand upload, the whole dock and the read-back"}
 
 
 def run_ours(a):
-    import numpy as np
     import torch
     from ud2b200 import Engine, GRID_F16, GRID_F32, MODE_GRID
     from ud2b200.batching import heuristic_opt_steps
+    from ud2b200.engine import pack_ligands, read_bandwidth
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -377,20 +563,27 @@ def run_ours(a):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     torch.cuda.set_device(local)
     nl = a.ligands
-    w, box, rec, ligs = make_inputs(a.workload, nl, a.seed, rank)
-    mc = a.mc_steps or w["mc_steps"]
-    opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
-    learned = a.mode == "learned"
-    tsets = train_sets(a.workload, a.train_ligands, (box.lo.astype(np.float64) + box.hi) / 2.0) if learned else []
-    mt = sorted(set(int(t) for l in list(ligs) + [x for ts in tsets for x in ts] for t in l.types if t != 0))
-    eng = Engine(box, device=local)
+    w, box, rec, _ = make_inputs(a.workload, 1, a.seed, rank)
+    center = (box.lo.astype(np.float64) + box.hi) / 2.0
     template = a.workload == "template"
+    from ud2b200 import synth
+    core = synth.make_core(center, a.seed) if template else None
+    mc = w["mc_steps"]                  # the gate reference's (and plain mode's) MC steps
+    learned = a.mode == "learned"
+    # fresh ligand batches: step k docks pool[k % P], P = min(steps, 3); each batch has its
+    # own seed (none shared with the training sets or the warm-up batch)
+    P = max(1, min(a.steps, a.pool))
+    pool = [ligand_batch(a.workload, nl, a.seed * 1000 + 11 * (j + 1), rank, center, core) for j in range(P)]
+    warm = ligand_batch(a.workload, nl, a.seed * 1000 + 7, rank, center, core)
+    tsets = train_sets(a.workload, a.train_ligands, center) if learned else []
+    opt = heuristic_opt_steps([l.natom for l in pool[0]], [l.ntors for l in pool[0]])
+    mt = sorted(set(int(t) for ls in pool + [warm] + tsets for l in ls for t in l.types if t != 0))
+    log(f"inputs ready: {P} fresh batches of {nl} ligands")
+    eng = Engine(box, device=local)
     if template:
-        # template-constrained screen: the shared core stays on its reference pose (no
-        # translation or rotation), every chain keeps 4 poses -> 1024 clustered per ligand
         eng.set_flags(constraint=True)
         eng.set_retain(4)
     eng.set_receptor(rec.xyz, rec.types)
@@ -398,130 +591,177 @@ def run_ours(a):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
     base_kw = dict(seed=a.seed, nchain=w["chains"], opt_steps=opt, refine_steps=5, num_pose=w["num_pose"],
                    rmsd_limit=w["rmsd"], energy_range=10.0, randomize=True, mode=MODE_GRID)
-    from ud2b200.engine import pack_ligands
-    packed = pack_ligands(ligs)
-    h2d = int(sum(v.nbytes for v in packed.values()))
     extra = {}
+    # the gate reference of every pool batch: the plain fused engine at the workload's MC
+    # steps (also the plain engine's throughput and end-to-end rate at full settings)
+    refs, ref_ms, ref_wall = [], [], []
     if learned:
-        # reference result and plain throughput: the fused engine at the workload's MC steps
-        eng.clear_ligands()
-        eng.add_ligands(ligs)
-        flush.fill_(0.0)
-        torch.cuda.synchronize()
-        res_ref, _ = eng.dock(**base_kw, mc_steps=mc, fetch=True)
-        st = eng.stage_times()
-        ref_scores = np.array(top_scores(res_ref))
-        plain_ms = float(st[5])
-        # proposal network trained on the GPU from the plain engine's own searches
+        for ls in pool:
+            res, ms, wall, _, _ = dock_timed(eng, ls, dict(base_kw, mc_steps=mc), flush)
+            refs.append(np.array(top_scores(res)))
+            ref_ms.append(ms)
+            ref_wall.append(wall)
+        log(f"gate references ({mc} MC steps): {[round(x / 1000, 1) for x in ref_ms]} s")
+        nref = nl * len(pool)
+        extra["plain"] = {"value": nref / (sum(ref_ms) / 1000.0), "unit": UNIT, "mc_steps": mc,
+                          "e2e": {"value": nref / sum(ref_wall), "unit": UNIT},
+                          "engine": "fused plain search (k_search) at the workload's MC steps: the gate reference"}
         from ud2b200.learned import train_proposal
         params, trep = train_proposal(box, rec, tsets, mt, opt_steps=opt, nchain=w["chains"], mc_steps=150,
                                       target=1, epochs=a.train_epochs, batch=1024, lr=1e-3, seed=1, device=local)
         eng.mlp_set_params(params)
-        # the method without the network: the fused plain engine at the learned engine's steps
-        res_eq, _ = eng.dock(**base_kw, mc_steps=a.learned_steps, fetch=True)
-        eq_ms = float(eng.stage_times()[5])
-        gap_eq = np.array(top_scores(res_eq)) - ref_scores
-        extra = {"plain": {"value": len(ligs) / (plain_ms / 1000.0), "unit": UNIT, "ms_per_step": plain_ms,
-                           "mc_steps": mc, "engine": "fused plain search (k_search)"},
-                 "learned_training": {"train_ligands": sum(len(t) for t in tsets), "ligand_seeds": [101, 102, 103, 104],
-                                      "samples": trep.samples, "collect_s": trep.collect_s, "train_s": trep.train_s,
-                                      "epoch_loss": trep.epoch_loss, "target": "move to the ligand's best pose"},
-                 "plain_equal_steps": {"value": len(ligs) / (eq_ms / 1000.0), "unit": UNIT, "mc_steps": a.learned_steps,
-                                       "within": float(np.mean(gap_eq <= 0.3)), "mean_gap": float(np.mean(gap_eq)),
-                                       "engine": "fused plain search at the learned engine's MC steps (untimed)"}}
-        run_kw = dict(base_kw, mc_steps=a.learned_steps)
+        log(f"network trained: {trep.samples} moves, {trep.collect_s:.1f} + {trep.train_s:.1f} s")
+        extra["learned_training"] = {"train_ligands": sum(len(t) for t in tsets), "ligand_seeds": [101, 102, 103, 104],
+                                     "samples": trep.samples, "collect_s": trep.collect_s, "train_s": trep.train_s,
+                                     "epoch_loss": trep.epoch_loss, "target": "move to the ligand's best pose"}
+        # step sweep of both engines on pool batch 0; each engine's gate step count is the
+        # smallest S whose share within 0.3 kcal/mol of the reference is >= 95 %
+        sweep = {"plain": [], "learned": []}
+        gate_s = {}
+        for eng_name, pl in (("plain", None), ("learned", a.p_learned)):
+            for S in [int(v) for v in a.sweep.split(",")]:
+                res, ms, _, _, _ = dock_timed(eng, pool[0], dict(base_kw, mc_steps=S), flush, p_learned=pl)
+                gap = np.array(top_scores(res)) - refs[0]
+                within = float(np.mean(gap <= 0.3))
+                sweep[eng_name].append({"mc_steps": S, "within": within, "mean_gap": float(np.mean(gap)),
+                                        "ligands_per_s": nl / (ms / 1000.0), "ms": ms})
+                if within >= 0.95 and eng_name not in gate_s:
+                    gate_s[eng_name] = S
+                elif eng_name in gate_s:
+                    break                      # one more S past the gate, then stop
+        log(f"sweep done: gate MC steps {gate_s}")
+        for k in ("plain", "learned"):
+            gate_s.setdefault(k, max(int(v) for v in a.sweep.split(",")))
+        # equal wall time: the plain engine's share within at the learned engine's time per batch
+        lt_s = arm_mc_steps(a, w)
+        lt = next((x["ms"] for x in sweep["learned"] if x["mc_steps"] == lt_s),
+                  next(x["ms"] for x in sweep["learned"] if x["mc_steps"] == gate_s["learned"]))
+        eq = [x for x in sweep["plain"] if x["ms"] <= lt * 1.02]
+        extra["sweep"] = {"batch": "pool batch 0", "p_learned": a.p_learned, "plain": sweep["plain"],
+                          "learned": sweep["learned"], "gate_mc_steps": gate_s,
+                          "equal_wall_time": {"learned_ms": lt, "plain": eq[-1] if eq else None}}
+        run_kw = dict(base_kw, mc_steps=arm_mc_steps(a, w))
         p_learned = a.p_learned
     else:
-        run_kw = dict(base_kw, mc_steps=mc)
+        run_kw = dict(base_kw, mc_steps=arm_mc_steps(a, w))
         p_learned = None
-    # warm-up steps dock the same batch through the same kernels with shorter chains
     warm_kw = dict(run_kw, mc_steps=min(run_kw["mc_steps"], a.warmup_mc_steps or run_kw["mc_steps"]))
-    dev_ms, e2e_s, stage, heavy, evals, launches = [], [], [], 0, 0, 0
+    dev_ms, e2e_s, stage, heavy, evals, launches, h2d, d2h = [], [], [], 0, 0, 0, 0, 0
+    gaps = []
     sampler = ClockSampler(local)
-    res = None
     for s in range(a.warmup + a.steps):
+        timed = s >= a.warmup
+        ls = pool[(s - a.warmup) % P] if timed else warm
         if s == a.warmup:
             torch.cuda.synchronize()
             if dist:
                 dist.barrier()
             sampler.__enter__()
-        flush.fill_(float(s))
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        eng.clear_ligands()
-        eng.add_ligands(ligs)
-        res, ne = eng.dock(**(run_kw if s >= a.warmup else warm_kw), fetch=True, p_learned=p_learned)
-        t1 = time.perf_counter()
-        st = eng.stage_times()
-        cn = eng.counters()
-        if s >= a.warmup:
-            dev_ms.append(float(st[5]))
-            e2e_s.append(t1 - t0)
-            stage.append(st.tolist())
+        res, ms, wall, cn, st = dock_timed(eng, ls, run_kw if timed else warm_kw, flush, p_learned=p_learned)
+        if timed:
+            dev_ms.append(ms)
+            e2e_s.append(wall)
+            stage.append(st)
             heavy += cn["heavy_atom_evaluations"]
             evals += cn["evaluations"]
             launches += cn["launches"]
+            h2d += int(sum(v.nbytes for v in pack_ligands(ls).values()))
+            d2h += int(sum(4 * (len(r.records) * (8 + 3 * l.natom + l.ntors) + 4 * len(r.records))
+                           for r, l in zip(res, ls)))
+            if learned:
+                gaps.append(np.array(top_scores(res)) - refs[(s - a.warmup) % P])
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     sampler.__exit__()
-    d2h = int(sum(4 * (len(r.records) * (8 + 3 * l.natom + l.ntors) + 4 * len(r.records)) for r, l in zip(res, ligs)))
-    tot_ms = sum(dev_ms)
-    tot_e2e = sum(e2e_s)
+    tot_ms, tot_e2e = sum(dev_ms), sum(e2e_s)
     search_ms = sum(x[0] for x in stage)
-    ligs_done = len(ligs) * a.steps
+    ligs_done = nl * a.steps
     if learned:
-        gap = np.array(top_scores(res)) - ref_scores
-        within = float(np.mean(gap <= 0.3))
+        g = np.concatenate(gaps)
+        within = float(np.mean(g <= 0.3))
         extra["quality"] = {"gap_kcal_mol": 0.3, "within": within, "gate": 0.95, "gate_met": within >= 0.95,
-                            "mean_gap": float(np.mean(gap)), "max_gap": float(np.max(gap)),
-                            "reference": f"plain fused search at {mc} MC steps, same batch, same seed"}
+                            "mean_gap": float(np.mean(g)), "max_gap": float(np.max(g)),
+                            "reference": f"plain fused search at {mc} MC steps on the same batch, same seed"}
+        # the plain engine at its own gate step count on the same batches
+        pms, pgap = [], []
+        for k in range(a.steps):
+            res, ms, _, _, _ = dock_timed(eng, pool[k % P], dict(base_kw, mc_steps=gate_s["plain"]), flush)
+            pms.append(ms)
+            pgap.append(np.array(top_scores(res)) - refs[k % P])
+        pg = np.concatenate(pgap)
+        extra["plain_at_gate"] = {"value": ligs_done / (sum(pms) / 1000.0), "unit": UNIT, "mc_steps": gate_s["plain"],
+                                  "within": float(np.mean(pg <= 0.3)), "mean_gap": float(np.mean(pg)),
+                                  "engine": "fused plain search at its smallest gate-passing MC steps, same batches"}
     if dist:
         tot_ms, tot_e2e, ligs_done = reduce_over_ranks(dist, tot_ms, tot_e2e, ligs_done, f"cuda:{local}")
     value = ligs_done / (tot_ms / 1000.0)
-    peak, peak_kind = load_peaks()
+    if learned:
+        extra["learned_vs_plain_at_gate"] = value / extra["plain_at_gate"]["value"]
+    hbm_peak, peak_kind = load_peaks()
+    peaks = {"hbm_gbs": hbm_peak, "l2_gbs": read_bandwidth(local, 32 << 20, 50),
+             "hbm_read_gbs": read_bandwidth(local, 4 << 30, 5)}
     bytes_alg = heavy * 8 * (2 if a.grid == "f16" else 4)
     achieved = bytes_alg / (search_ms / 1000.0) / 1e9 if search_ms > 0 else 0.0
-    # launches of the dominant kernel per step: k_search runs a dock's search in one launch,
-    # k_learn_step one MC step of every chain per launch
     launches_per_step = run_kw["mc_steps"] if learned else 1
     tr = load_traffic("k_learn_step_screen.md" if learned else "k_search_screen.md")
-    traffic = tr if (tr is not None and nl == 148 and a.workload == "screen" and a.grid == "f32"
-                     and (learned or mc == w["mc_steps"])) else None
+    traffic = tr if (tr is not None and nl == 148 and a.workload == "screen" and a.grid == "f32") else None
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": tot_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f32", "data": "synthetic",
-           "config": {"workload": a.workload, "engine": "learned proposal" if learned else "fused plain search",
-                      "ligands_per_step_per_gpu": len(ligs), "chains": w["chains"], "mc_steps": run_kw["mc_steps"],
-                      "p_learned": p_learned, "opt_steps": opt, "refine_steps": 5, "num_pose": w["num_pose"],
-                      "rmsd_limit": w["rmsd"], "receptor_atoms": rec.natom, "box_A": w["box"], "grid_spacing_A": 0.375,
-                      "grid_maps": len(mt), "grid_precision": a.grid, "l2": "flushed between steps (256 MB write)",
-                      "constraint_docking": template, "poses_kept_per_chain": 4 if template else 1,
-                      "warmup": f"{a.warmup} steps, same batch, {warm_kw['mc_steps']} MC steps per chain",
-                      "parallelism": f"ligand shards x{world}"},
-           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": traffic,
+           "config": workload_config(a, w, rec, opt, run_kw["mc_steps"], P, world),
+           "engine_config": {"engine": "learned proposal" if learned else "fused plain search",
+                             "p_learned": p_learned, "grid_maps": len(mt), "grid_precision": a.grid,
+                             "warmup": f"{a.warmup} steps on a separate batch, {warm_kw['mc_steps']} MC steps"},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak, "traffic": traffic,
                         "kernel": "k_learn_step" if learned else "k_search",
                         "peak_kind": f"{peak_kind} hbm copy bandwidth",
                         "algorithmic_bytes_per_launch": bytes_alg / a.steps / launches_per_step,
-                        "launches_per_step": launches_per_step},
-           "e2e": {"value": ligs_done / tot_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                        "launches_per_step": launches_per_step,
+                        "traffic_source": "DRAM bytes per launch from the committed ncu capture of this kernel on the "
+                                          "148-ligand screen batch (profiles/); null when the run's shape differs",
+                        "l2": {"achieved": achieved, "peak": peaks["l2_gbs"], "frac": achieved / peaks["l2_gbs"],
+                               "peak_kind": "measured in this run: streaming reads of a 32 MB buffer"}},
+           "peaks_measured_here": peaks,
+           "e2e": {"value": ligs_done / tot_e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // a.steps,
+                   "d2h_bytes_per_step": d2h // a.steps},
            "gpu_launches": launches,
            "stage_ms_per_step": [sum(x[i] for x in stage) / a.steps for i in range(6)],
            "evaluations_per_step": evals / a.steps,
            "poses_scored_per_s": evals / (search_ms / 1000.0) if search_ms > 0 else None,
            "clocks": sampler.summary()}
     out.update(extra)
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        rate, cores, sample = cpu_port_rate(w, box, rec, ligs, mc, opt, a.cpu_seconds)
-        out["cpu_baseline"] = {"value": rate / (w["chains"] * mc), "unit": UNIT, "cores": cores, "kind": "port",
-                               "sample": sample + f"; ligands/s at {mc} MC steps per chain"}
-        ref_sc = reference_scoring_rate(rec, box, ligs)
-        if ref_sc:
-            out["reference_cpu_scoring"] = ref_sc
+    log(f"timed steps done: {value:.3f} ligands/s")
+
+    def block(name, fn):
+        # an extra measurement that fails is recorded, not fatal to the line
+        try:
+            t = time.perf_counter()
+            r = fn()
+            log(f"{name}: {time.perf_counter() - t:.1f} s")
+            if r is not None:
+                out[name] = r
+        except Exception as e:          # noqa: BLE001
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+            log(f"{name} failed: {e}")
+
+    if rank == 0 and world == 1:
+        block("k_score_roofline", lambda: kscore_roofline(eng, pool[0], peaks, a.grid))
     eng.close()
+    if rank == 0 and world == 1 and not a.no_extras:
+        block("uneven_65536", lambda: uneven_full(a, w, box, rec, local))
+        block("reference_gpu", lambda: run_reference_gpu(a, emit=False))
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        def cpu():
+            m = run_kw["mc_steps"]
+            rate, cores, sample = cpu_port_rate(w, box, rec, pool[0], m, opt, a.cpu_seconds)
+            return {"value": rate / (w["chains"] * m), "unit": UNIT, "cores": cores, "kind": "port",
+                    "sample": sample + f"; ligands/s at {m} MC steps per chain (this arm's)"}
+        block("cpu_baseline", cpu)
+        block("reference_cpu_scoring", lambda: reference_scoring_rate(rec, box, pool[0]))
     if rank == 0:
-        print(json.dumps(out), flush=True)
+        emit_line(out)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

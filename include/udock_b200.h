@@ -165,9 +165,10 @@ int ud_score_batch_noalloc(ud_ctx* ctx, int n, const int* pose_lig, const float*
                            const float* rotvecs, int mode, float vcap, float slope, float* out_e, float* out_g);
 
 /* Measurement helpers (used by bench.py for the roofline; not part of the reference path).
- * ud_read_bandwidth: streaming 16-byte reads of a `bytes` buffer, `repeats` times after 3
- * warm-up passes, timed with CUDA events: the L2 read bandwidth when the buffer fits the
- * L2 (126 MB on B200), the HBM read bandwidth when it is far larger.
+ * ud_read_bandwidth: streaming 16-byte reads of a `bytes` buffer (each launch reads it as
+ * many times as make at least 1 GiB), `repeats` launches after 3 warm-up ones, timed with
+ * CUDA events: the L2 read bandwidth when the buffer fits the L2 (126 MB on B200), the HBM
+ * read bandwidth when it is far larger.
  * ud_score_batch_timed: ud_score_batch with the inputs uploaded once and the scoring
  * kernel launched `repeats` times back to back (after one warm-up launch); out_ms is the
  * mean kernel time.  Results as ud_score_batch.  No counterpart in the reference. */

@@ -1,5 +1,6 @@
 """The multi-GPU path of bench.py on CPU: two gloo ranks shard the ligands (disjoint
-ligands, the same receptor) and reduce the timings (max over ranks, ligands summed)."""
+ligands in every fresh batch, the same receptor) and reduce the timings (max over ranks,
+ligands summed)."""
 import os
 import socket
 import sys
@@ -27,7 +28,10 @@ def _rank(rank, world, port, out):
     try:
         import bench
         w, box, rec, ligs = bench.make_inputs("small", 3, 1, rank)
-        names = [l.name for l in ligs]
+        center = (box.lo.astype(np.float64) + box.hi) / 2.0
+        # the timed steps' fresh batches, as run_ours builds them on each rank
+        pool = [bench.ligand_batch("small", 3, 1000 + 11 * (j + 1), rank, center) for j in range(2)]
+        names = [l.name for l in ligs] + [l.name for b in pool for l in b]
         rec_sum = hashlib.sha1(np.ascontiguousarray(rec.xyz).tobytes()).hexdigest()
         gathered = [None] * world
         dist.all_gather_object(gathered, (names, rec_sum))
@@ -53,5 +57,5 @@ def test_two_ranks_shard_and_reduce():
     (names0, rec0), (names1, rec1) = gathered
     assert rec0 == rec1                                  # every rank docks against the same receptor
     assert not set(names0) & set(names1)                 # ligand shards are disjoint
-    assert len(names0) == len(names1) == 3
+    assert len(names0) == len(names1) == 9
     assert dev_ms == 200.0 and e2e_s == 2.0 and n == 6   # slowest rank's times, all ranks' ligands

@@ -193,13 +193,15 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
 // Streaming read of a buffer (16-byte loads, grid-stride), summed so the loads are kept;
 // one partial sum per thread block.  With a buffer that fits the L2 the repeated reads are
 // L2 hits (the L2 read bandwidth); with one far larger, HBM reads.
-__global__ void __launch_bounds__(512) k_read_probe(const float4* __restrict__ buf, long long n4, float* out) {
+__global__ void __launch_bounds__(512) k_read_probe(const float4* __restrict__ buf, long long n4, int passes,
+                                                    float* out) {
     float s = 0.f;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
-        const float4 v = __ldcg(buf + i);
-        s += (v.x + v.y) + (v.z + v.w);
-    }
+    for (int r = 0; r < passes; r++)
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+            const float4 v = __ldcg(buf + i);
+            s += (v.x + v.y) + (v.z + v.w);
+        }
     s = warp_sum(s);
     if ((threadIdx.x & 31) == 0) atomicAdd(out + blockIdx.x, s);
 }
@@ -1772,9 +1774,11 @@ int ud_read_bandwidth(int device, long long bytes, int repeats, float* out_gbps)
         ck(cudaEventCreate(&e1), "event");
         ck(cudaMemsetAsync(buf.p, 0, (size_t)n4 * 16, st), "memset");
         ck(cudaMemsetAsync(part.p, 0, (size_t)grid * 4, st), "memset");
-        for (int w = 0; w < 3; w++) k_read_probe<<<grid, 512, 0, st>>>(buf.p, n4, part.p);
+        // enough passes per launch that a launch reads at least 1 GiB (launch overhead negligible)
+        const int passes = (int)std::max<long long>(1, (1LL << 30) / ((long long)n4 * 16));
+        for (int w = 0; w < 3; w++) k_read_probe<<<grid, 512, 0, st>>>(buf.p, n4, passes, part.p);
         ck(cudaEventRecord(e0, st), "event");
-        for (int r = 0; r < repeats; r++) k_read_probe<<<grid, 512, 0, st>>>(buf.p, n4, part.p);
+        for (int r = 0; r < repeats; r++) k_read_probe<<<grid, 512, 0, st>>>(buf.p, n4, passes, part.p);
         ck(cudaEventRecord(e1, st), "event");
         ck(cudaGetLastError(), "k_read_probe launch");
         ck(cudaEventSynchronize(e1), "probe");
@@ -1783,7 +1787,7 @@ int ud_read_bandwidth(int device, long long bytes, int repeats, float* out_gbps)
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         cudaStreamDestroy(st);
-        *out_gbps = (float)((double)n4 * 16.0 * repeats / (ms * 1e-3) / 1e9);
+        *out_gbps = (float)((double)n4 * 16.0 * passes * repeats / (ms * 1e-3) / 1e9);
         return UD_OK;
     } catch (const Fail& f) {
         return fail(f);
