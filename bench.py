@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--p-learned", type=float, default=0.25, help="share of learned moves")
     ap.add_argument("--train-ligands", type=int, default=37, help="training ligands per seed (4 seeds)")
     ap.add_argument("--train-epochs", type=int, default=6, help="epochs of network training")
+    ap.add_argument("--ref-steps", type=int, default=0,
+                    help="MC steps of the gate reference (0 = the workload's; smaller only for profiling runs)")
     ap.add_argument("--pool", type=int, default=3, help="fresh ligand batches the timed steps cycle through")
     ap.add_argument("--sweep", default="50,100,200,400,1000", help="MC steps of the step sweep")
     ap.add_argument("--no-extras", action="store_true", help="skip the 65,536-ligand and reference-engine blocks")
@@ -571,7 +573,7 @@ def run_ours(a):
     template = a.workload == "template"
     from ud2b200 import synth
     core = synth.make_core(center, a.seed) if template else None
-    mc = w["mc_steps"]                  # the gate reference's (and plain mode's) MC steps
+    mc = a.ref_steps or w["mc_steps"]   # the gate reference's MC steps
     learned = a.mode == "learned"
     # fresh ligand batches: step k docks pool[k % P], P = min(steps, 3); each batch has its
     # own seed (none shared with the training sets or the warm-up batch)
