@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--p-learned", type=float, default=0.25, help="share of learned moves")
     ap.add_argument("--train-ligands", type=int, default=37, help="training ligands per seed (4 seeds)")
     ap.add_argument("--train-epochs", type=int, default=6, help="epochs of network training")
+    ap.add_argument("--train-moves", type=int, default=1_500_000,
+                    help="moves recorded for training (smaller only for profiling runs)")
     ap.add_argument("--ref-steps", type=int, default=0,
                     help="MC steps of the gate reference (0 = the workload's; smaller only for profiling runs)")
     ap.add_argument("--pool", type=int, default=3, help="fresh ligand batches the timed steps cycle through")
@@ -610,7 +612,8 @@ def run_ours(a):
                           "engine": "fused plain search (k_search) at the workload's MC steps: the gate reference"}
         from ud2b200.learned import train_proposal
         params, trep = train_proposal(box, rec, tsets, mt, opt_steps=opt, nchain=w["chains"], mc_steps=150,
-                                      target=1, epochs=a.train_epochs, batch=1024, lr=1e-3, seed=1, device=local)
+                                      target=1, epochs=a.train_epochs, batch=1024, lr=1e-3, seed=1, device=local,
+                                      max_moves=a.train_moves)
         eng.mlp_set_params(params)
         log(f"network trained: {trep.samples} moves, {trep.collect_s:.1f} + {trep.train_s:.1f} s")
         extra["learned_training"] = {"train_ligands": sum(len(t) for t in tsets), "ligand_seeds": [101, 102, 103, 104],
