@@ -308,8 +308,9 @@ int ud_search_shape(const ud_ctx* ctx, int* out4);
  * W3[256x256], b3, W4[256x64], b4; W row-major [in x out].  Output row (64): mean[0:26],
  * raw log-variance[26:52] (clamped to [-8, 4] where used), 12 unused. */
 long long ud_mlp_param_count(void);
-/* Tensor-core path of the network's forward pass: 1 = tcgen05.mma with a tensor-memory
- * accumulator (default), 0 = mma.sync (the backward pass always uses mma.sync). */
+/* Tensor-core path of the network's GEMMs (forward pass and the training backward pass):
+ * 1 = tcgen05.mma with a tensor-memory accumulator (default; the backward contracts over the
+ * batch through transposed operands), 0 = mma.sync. */
 int ud_mlp_set_gemm(ud_ctx* ctx, int kind);
 /* He-normal weights (last layer scaled by 0.1), zero biases, Adam state cleared. */
 int ud_mlp_init(ud_ctx* ctx, uint64_t seed);

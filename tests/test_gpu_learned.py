@@ -97,6 +97,35 @@ def test_loss_and_gradient_match_oracle(bare_engine):
         off += n
 
 
+@pytest.mark.parametrize("n", [130, 1024])
+def test_tcgen05_backward_matches_mma_sync(bare_engine, n):
+    """The training contraction on tcgen05 (weight gradients h^T d over the batch, padded to a
+    multiple of 32; input gradients d W^T through transposed weights) against the mma.sync
+    backward on the same BF16 operands: every gradient block within 1e-2 of its norm, and both
+    within the oracle's 3e-2."""
+    rng = np.random.default_rng(12)
+    p = M.init_params(13)
+    p = (p + rng.normal(0, 0.01, p.size)).astype(np.float32)
+    bare_engine.mlp_set_params(p)
+    X, Y, Mk = _data(rng, n)
+    bare_engine.mlp_set_gemm(1)
+    l_tc, g_tc = bare_engine.mlp_loss_grad(X, Y, Mk)
+    bare_engine.mlp_set_gemm(0)
+    try:
+        l_ms, g_ms = bare_engine.mlp_loss_grad(X, Y, Mk)
+    finally:
+        bare_engine.mlp_set_gemm(1)
+    want_loss, want_g = M.loss_grad(p, X, Y, Mk)
+    assert abs(l_tc - l_ms) <= 1e-3 * max(1.0, abs(l_ms))
+    off = 0
+    for shape in M.SHAPES:
+        k = int(np.prod(shape))
+        a, b, w = (v[off:off + k].astype(np.float64) for v in (g_tc, g_ms, want_g))
+        assert np.linalg.norm(a - b) <= 1e-2 * max(np.linalg.norm(b), 1e-12), shape
+        assert np.linalg.norm(a - w) <= 3e-2 * max(np.linalg.norm(w), 1e-12), shape
+        off += k
+
+
 def test_training_lowers_loss(bare_engine):
     rng = np.random.default_rng(3)
     X, _, Mk = _data(rng, 2048)

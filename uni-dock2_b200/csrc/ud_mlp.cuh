@@ -192,6 +192,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
                            ((uint32_t)(TC_BM >> 4) << 24);
     const int nstage = K / TC_BK;
     const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
+    int issued = -1;                                       // last stage whose MMAs were committed
     for (int s = 0; s < nstage; s++) {
         const int b = s & 1;
         if (s >= 2) {
@@ -232,11 +233,14 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          :: "r"(smem_u32(&bars[b])) : "memory");
         }
+        issued = s;
     }
-    // all MMAs done when the last stage's barrier phase completes
-    if (!s_fail && nstage > 0) {
-        const int last = nstage - 1;
-        if (!mbar_wait(smem_u32(&bars[last & 1]), (uint32_t)((last >> 1) & 1))) { if (tid == 0) s_fail = 1; }
+    // all MMAs done when the barrier phase of the last committed stage completes (a commit
+    // tracks every MMA issued before it).  Also after a timed-out wait above, so that tensor
+    // memory is not freed under MMAs still in flight; if this bounded wait times out as well,
+    // what the tensor cores still do with the released columns is undefined.
+    if (issued >= 0) {
+        if (!mbar_wait(smem_u32(&bars[issued & 1]), (uint32_t)((issued >> 1) & 1))) { if (tid == 0) s_fail = 1; }
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -275,6 +279,25 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(N) : "memory");
+}
+
+// out[c * ldo + r] = in[r * C + c] for r < R, c < C, and 0 for R <= r < ldo: a BF16 transpose
+// through 32 x 32 shared-memory tiles (block 32 x 8), zero-padding the new rows' tails so they can
+// serve as the K-extended operand of a tensor-core GEMM
+__global__ void __launch_bounds__(256) k_transpose_bf16(const __nv_bfloat16* __restrict__ in, int R, int C,
+                                                        __nv_bfloat16* __restrict__ out, int ldo) {
+    __shared__ __nv_bfloat16 tile[32][34];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        tile[i][threadIdx.x] = (r < R && c < C) ? in[(long long)r * C + c] : zero;
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (c < C && r < ldo) out[(long long)c * ldo + r] = tile[threadIdx.x][i];
+    }
 }
 
 __global__ void k_f32_to_bf16(long long n, const float* __restrict__ s, __nv_bfloat16* __restrict__ d) {

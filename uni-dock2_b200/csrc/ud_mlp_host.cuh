@@ -9,22 +9,26 @@ struct MlpState {
     bool ready = false;
     int adam_t = 0;
     int cap = 0;
-    bool use_tc = true;                     // forward pass on tcgen05 (else mma.sync)
+    bool use_tc = true;                     // forward and backward GEMMs on tcgen05 (else mma.sync)
     bool tc_attr = false;
     DBuf<int> tc_err;                       // set by a tcgen05 GEMM whose wait timed out
     DBuf<float> p, g, m, v;                 // NPARAM each
     DBuf<__nv_bfloat16> p16;
-    DBuf<__nv_bfloat16> x16, h16[3], d16;   // activations of up to cap rows
+    DBuf<__nv_bfloat16> x16, h16[3], d16;   // activations of up to cap rows (d16: cap rounded up to 32)
+    DBuf<__nv_bfloat16> xt16, wt16;         // tcgen05 backward: an activation transposed, a weight transposed
     DBuf<float> out, dout, dh, dpre;
     DBuf<double> loss;
 
     static int blocks(long long n) { return (int)std::min<long long>((n + 255) / 256, 4096); }
+    static int pad32(int n) { return (n + 31) & ~31; }
 
     void ensure(int n) {
         if (n <= cap) return;
         x16.ensure((size_t)n * mlp::IN);
         for (auto& h : h16) h.ensure((size_t)n * mlp::HID);
-        d16.ensure((size_t)n * mlp::HID);
+        d16.ensure((size_t)pad32(n) * mlp::HID);
+        xt16.ensure((size_t)mlp::IN * pad32(n));
+        wt16.ensure((size_t)mlp::HID * mlp::HID);
         out.ensure((size_t)n * mlp::OUT);
         dout.ensure((size_t)n * mlp::OUT);
         dh.ensure((size_t)n * mlp::HID);
@@ -127,6 +131,62 @@ struct MlpState {
              0, p.p + mlp::OFF_B4, 0);
     }
 
+    // in [R x C] (BF16, row-major) -> out [C x ldo], rows zero-padded from R to ldo
+    static void transpose(cudaStream_t s, const __nv_bfloat16* in, int R, int C, __nv_bfloat16* out, int ldo) {
+        dim3 grid((unsigned)((C + 31) / 32), (unsigned)((ldo + 31) / 32));
+        k_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(in, R, C, out, ldo);
+        ck(cudaGetLastError(), "k_transpose_bf16");
+    }
+
+    // Y[M x N] (FP32) = X[M x K] W[K x N] on the tensor cores, no bias or activation
+    void tc_gemm(cudaStream_t s, const __nv_bfloat16* X, int M, int K, const __nv_bfloat16* W, int N, float* Y) {
+        const unsigned grid = (unsigned)((M + TC_BM - 1) / TC_BM);
+        if (N == 256)
+            k_gemm_tc<256><<<grid, 128, TC_SMEM, s>>>(X, W, nullptr, M, K, 0, nullptr, Y, tc_err.p);
+        else
+            k_gemm_tc<64><<<grid, 128, TC_SMEM, s>>>(X, W, nullptr, M, K, 0, nullptr, Y, tc_err.p);
+        ck(cudaGetLastError(), "k_gemm_tc");
+    }
+
+    // The backward products on tcgen05.  Weight gradients dW = h_in^T d contract over the batch:
+    // h_in is transposed into [K_in x n32] (n32 = n rounded up to 32, zero tail) and d16 holds
+    // n32 rows with a zero tail, so K = n32 meets the kernel's multiple-of-32 rule.  Input
+    // gradients dh = d W^T take W transposed into [N_out x K_in].
+    void backward_tc(cudaStream_t s, int n, const __nv_bfloat16* x) {
+        prepare(s);
+        const int n32 = pad32(n);
+        const __nv_bfloat16* w = p16.p;
+        // d16 rows n..n32 (in both the 64- and the 256-wide views) stay zero
+        if (n32 > n)
+            ck(cudaMemsetAsync(d16.p + (size_t)n * mlp::OUT, 0, ((size_t)n32 * mlp::HID - (size_t)n * mlp::OUT) * 2, s),
+               "memset");
+        const long long no = (long long)n * mlp::OUT;
+        k_f32_to_bf16<<<blocks(no), 256, 0, s>>>(no, dout.p, d16.p);
+        // output layer: dW4 = h3^T d [256 x 64], db4 = colsum(d), dh3 = d W4^T [n x 256]
+        transpose(s, h16[2].p, n, mlp::HID, xt16.p, n32);
+        tc_gemm(s, xt16.p, mlp::HID, n32, d16.p, mlp::OUT, g.p + mlp::OFF_W4);
+        k_colsum<<<1, 64, 0, s>>>(n, mlp::OUT, dout.p, g.p + mlp::OFF_B4);
+        transpose(s, w + mlp::OFF_W4, mlp::HID, mlp::OUT, wt16.p, mlp::HID);
+        tc_gemm(s, d16.p, n, mlp::OUT, wt16.p, mlp::HID, dh.p);
+        const long long off_w[3] = {mlp::OFF_W1, mlp::OFF_W2, mlp::OFF_W3};
+        const long long off_b[3] = {mlp::OFF_B1, mlp::OFF_B2, mlp::OFF_B3};
+        const long long nh = (long long)n * mlp::HID;
+        for (int l = 2; l >= 0; l--) {
+            k_relu_bwd<<<blocks(nh), 256, 0, s>>>(nh, dh.p, h16[l].p, dpre.p, d16.p);
+            ck(cudaGetLastError(), "k_relu_bwd");
+            const __nv_bfloat16* hin = l ? h16[l - 1].p : x;
+            const int kin = l ? mlp::HID : mlp::IN;
+            transpose(s, hin, n, kin, xt16.p, n32);
+            tc_gemm(s, xt16.p, kin, n32, d16.p, mlp::HID, g.p + off_w[l]);
+            k_colsum<<<1, 256, 0, s>>>(n, mlp::HID, dpre.p, g.p + off_b[l]);
+            if (l > 0) {
+                transpose(s, w + off_w[l], mlp::HID, mlp::HID, wt16.p, mlp::HID);
+                tc_gemm(s, d16.p, n, mlp::HID, wt16.p, mlp::HID, dh.p);
+            }
+        }
+        ck(cudaGetLastError(), "mlp backward");
+    }
+
     // gradients of the mean NLL into g (after forward on x); the batch's mean loss is
     // added to loss.p[0] (cleared first when reset)
     void loss_backward(cudaStream_t s, int n, const __nv_bfloat16* x, const float* Y, const float* M, bool reset) {
@@ -135,6 +195,10 @@ struct MlpState {
         const long long no = (long long)n * mlp::OUT;
         k_mlp_nll<<<(int)((no + 255) / 256), 256, 0, s>>>(n, out.p, Y, M, dout.p, loss.p);
         ck(cudaGetLastError(), "k_mlp_nll");
+        if (use_tc) {
+            backward_tc(s, n, x);
+            return;
+        }
         const __nv_bfloat16* w = p16.p;
         // output layer: dW4 = h3^T d, db4 = colsum(d), dh3 = d W4^T
         k_f32_to_bf16<<<blocks(no), 256, 0, s>>>(no, dout.p, d16.p);

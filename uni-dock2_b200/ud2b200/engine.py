@@ -367,7 +367,7 @@ class Engine:
         return int(self.L.ud_mlp_param_count())
 
     def mlp_set_gemm(self, kind: int):
-        """Forward pass on tcgen05 (1, default) or mma.sync (0)."""
+        """Network GEMMs (forward and training backward) on tcgen05 (1, default) or mma.sync (0)."""
         self._check(self.L.ud_mlp_set_gemm(self.h, int(kind)))
 
     def mlp_init(self, seed: int = 0):
