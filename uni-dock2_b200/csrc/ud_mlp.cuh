@@ -8,6 +8,7 @@
 // weights, hidden activations and back-propagated pre-activation gradients; FP32 sums,
 // biases, loss and optimiser) are restated in oracle/mlp_oracle.py.
 #pragma once
+#include <cuda.h>          // CUtensorMap (the TMA descriptor; encoded on the host at run time)
 #include <cuda_bf16.h>
 #include <random>
 
@@ -122,16 +123,23 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
                 }
 }
 
-// ---------------------------------------------------------------------- tcgen05 forward GEMM
+// ---------------------------------------------------------------------- tcgen05 GEMM, TMA-staged
 // Y[M x N] = act(X[M x K] W[K x N] + b) on the 5th-generation tensor cores: one CTA of 128
 // threads per 128-row tile, the FP32 accumulator (128 lanes x N columns) in tensor memory,
 // one thread issuing tcgen05.mma (kind::f16, BF16 operands, M = 128, K = 16 per instruction).
-// Operands are staged 32 K-values at a time, double buffered, in the canonical no-swizzle
-// layouts: X K-major (8 rows x 16 bytes per core matrix), W N-major (8 K-rows x 8 N-values per
-// core matrix), both loaded with 16-byte vector loads.  Each stage's MMAs are committed to
-// that buffer's mbarrier; the buffer is refilled only after its barrier phase completes.
-// Every wait is bounded: on timeout the kernel records an error and skips to the release of
-// its tensor memory.  N is 64 or 256, K a multiple of 32; rows beyond M are zero-filled.
+// Operands arrive 32 K-values at a time by TMA (cp.async.bulk.tensor, no multicast), double
+// buffered: while the tensor cores work on one stage the next stage's tiles are loading.  The
+// canonical no-swizzle layouts come straight out of 3-D tensor maps:
+//  * X (K-major): dims (8 k, rows, K/8 chunks), strides (ld*2 B, 16 B), box (8, 128, 4): four
+//    2 KB chunk blocks of 128 rows x 16 B; core matrices K-adjacent 2048 B apart, M-adjacent
+//    128 B apart;
+//  * W (N-major): dims (8 n, K rows, N/8 chunks), strides (N*2 B, 16 B), box (8, 32, N/8): N/8
+//    blocks of 32 k-rows x 16 B; core matrices K-adjacent 128 B, N-adjacent 512 B apart.
+// Rows beyond the map's extent arrive as zeros.  Split-K: grid.y CTAs share a tile's K range
+// (kchunk each) and write FP32 partials [split][M][N], summed by k_sum_splits in split order.
+// Every wait is bounded: on timeout the kernel records an error, waits (bounded) for its own
+// copies and MMAs in flight, and releases its tensor memory.  N is 64 or 256, kchunk a
+// multiple of 32.
 constexpr int TC_BM = 128, TC_BK = 32;
 constexpr long long TC_SPIN = 1LL << 26;
 
@@ -155,9 +163,18 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
+// one 3-D tile of a tensor map into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :: "r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(bar)
+        : "memory");
+}
+
 template <int N>
-__global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ Wt,
-                                                 const float* __restrict__ bias, int M, int K, int relu,
+__global__ void __launch_bounds__(128) k_gemm_tc(const __grid_constant__ CUtensorMap tmX,
+                                                 const __grid_constant__ CUtensorMap tmW,
+                                                 const float* __restrict__ bias, int M, int kchunk, int relu,
                                                  __nv_bfloat16* __restrict__ Y16, float* __restrict__ Y32, int* err) {
     static_assert(N == 64 || N == 256, "N");
     constexpr int A_BYTES = TC_BM * TC_BK * 2;              // 8 KB per stage
@@ -167,21 +184,25 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
     unsigned char* tc_smem = tc_smem_raw + ((1024u - (smem_u32(tc_smem_raw) & 1023u)) & 1023u);
     unsigned char* sA[2] = {tc_smem, tc_smem + A_BYTES};
     unsigned char* sB[2] = {tc_smem + 2 * A_BYTES, tc_smem + 2 * A_BYTES + B_BYTES};
-    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ __align__(8) uint64_t mma_bar[2], tma_bar[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_fail;
+    __shared__ int s_fail, s_issued;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * TC_BM;
+    const int kbase = blockIdx.y * kchunk;
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(smem_u32(&s_tmem)), "r"(N) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[1])) : "memory");
+        for (int i = 0; i < 2; i++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mma_bar[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&tma_bar[i])) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
+        s_issued = -1;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -190,39 +211,39 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
     // instruction descriptor: F32 accumulate, BF16 A and B, A K-major, B N-major, N, M = 128
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
                            ((uint32_t)(TC_BM >> 4) << 24);
-    const int nstage = K / TC_BK;
-    const uint4 zero4 = make_uint4(0u, 0u, 0u, 0u);
-    int issued = -1;                                       // last stage whose MMAs were committed
-    for (int s = 0; s < nstage; s++) {
-        const int b = s & 1;
-        if (s >= 2) {
-            if (!mbar_wait(smem_u32(&bars[b]), (uint32_t)(((s - 2) >> 1) & 1))) { if (tid == 0) s_fail = 1; }
-            __syncthreads();
-            if (s_fail) break;
-        }
-        const int k0 = s * TC_BK;
-        // X tile: row m, 8 consecutive k per 16-byte vector; K-major core matrices
-        for (int v = tid; v < TC_BM * (TC_BK / 8); v += 128) {
-            const int r = v >> 2, kc = v & 3;                  // kc: 8-wide k chunk 0..3
-            const int m = m0 + r;
-            const uint4 val = m < M ? *reinterpret_cast<const uint4*>(X + (long long)m * K + k0 + kc * 8) : zero4;
-            const int step = kc >> 1, half = kc & 1;
-            *reinterpret_cast<uint4*>(sA[b] + step * (TC_BM / 8) * 256 + (r >> 3) * 256 + half * 128 + (r & 7) * 16) = val;
-        }
-        // W tile: k row, 8 consecutive n per 16-byte vector; N-major core matrices
-        for (int v = tid; v < TC_BK * (N / 8); v += 128) {
-            const int kk = v / (N / 8), nc = v % (N / 8);
-            const uint4 val = *reinterpret_cast<const uint4*>(Wt + (long long)(k0 + kk) * N + nc * 8);
-            const int step = kk >> 4, kg = (kk >> 3) & 1, kr = kk & 7;
-            *reinterpret_cast<uint4*>(sB[b] + step * (N / 8) * 256 + kg * (N / 8) * 128 + nc * 128 + kr * 16) = val;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+    const int nstage = kchunk / TC_BK;
+    if (tid == 0) {
+        int loaded = 0, consumed = 0, issued = -1;
+        bool fail = false;
+        auto load = [&](int s) {
+            const int b = s & 1;
+            const int k0 = kbase + s * TC_BK;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         :: "r"(smem_u32(&tma_bar[b])), "r"((uint32_t)(A_BYTES + B_BYTES)) : "memory");
+            tma_load_3d(sA[b], &tmX, 0, m0, k0 >> 3, smem_u32(&tma_bar[b]));
+            tma_load_3d(sB[b], &tmW, 0, k0, 0, smem_u32(&tma_bar[b]));
+        };
+        if (nstage > 0) { load(0); loaded = 1; }
+        for (int s = 0; s < nstage && !fail; s++) {
+            const int b = s & 1;
+            if (s + 1 < nstage) {
+                // the other buffer held stage s - 1: its MMAs finish before it is refilled
+                if (s >= 1 && !mbar_wait(smem_u32(&mma_bar[(s - 1) & 1]), (uint32_t)(((s - 1) >> 1) & 1))) {
+                    fail = true;
+                    break;
+                }
+                load(s + 1);
+                loaded = s + 2;
+            }
+            if (!mbar_wait(smem_u32(&tma_bar[b]), (uint32_t)((s >> 1) & 1))) {
+                fail = true;
+                break;
+            }
+            consumed = s + 1;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             for (int step = 0; step < TC_BK / 16; step++) {
-                const uint64_t da = umma_desc(smem_u32(sA[b] + step * (TC_BM / 8) * 256), 128, 256);
-                const uint64_t db = umma_desc(smem_u32(sB[b] + step * (N / 8) * 256), (N / 8) * 128, 128);
+                const uint64_t da = umma_desc(smem_u32(sA[b] + step * 2 * 2048), 2048, 128);
+                const uint64_t db = umma_desc(smem_u32(sB[b] + step * 256), 128, 512);
                 const uint32_t acc = (s > 0 || step > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
@@ -231,21 +252,30 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
                     :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u) : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         :: "r"(smem_u32(&bars[b])) : "memory");
+                         :: "r"(smem_u32(&mma_bar[b])) : "memory");
+            issued = s;
         }
-        issued = s;
+        if (fail) {
+            // copies still in flight land before the buffers are released (bounded)
+            for (int t = consumed; t < loaded; t++) mbar_wait(smem_u32(&tma_bar[t & 1]), (uint32_t)((t >> 1) & 1));
+            s_fail = 1;
+        }
+        s_issued = issued;
     }
+    __syncthreads();
     // all MMAs done when the barrier phase of the last committed stage completes (a commit
-    // tracks every MMA issued before it).  Also after a timed-out wait above, so that tensor
-    // memory is not freed under MMAs still in flight; if this bounded wait times out as well,
-    // what the tensor cores still do with the released columns is undefined.
-    if (issued >= 0) {
-        if (!mbar_wait(smem_u32(&bars[issued & 1]), (uint32_t)((issued >> 1) & 1))) { if (tid == 0) s_fail = 1; }
+    // tracks every MMA issued before it); also after a timeout, so that tensor memory is not
+    // released under MMAs still in flight; if this bounded wait times out as well, what the
+    // tensor cores still do with the released columns is undefined
+    const int issued = s_issued;
+    if (issued >= 0 && !mbar_wait(smem_u32(&mma_bar[issued & 1]), (uint32_t)((issued >> 1) & 1))) {
+        if (tid == 0) s_fail = 1;
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!s_fail) {
+    if (!s_fail && issued == nstage - 1) {
         const int m = m0 + warp * 32 + lane;                   // this thread's row (TMEM lane)
+        float* Yp = Y32 ? Y32 + (size_t)blockIdx.y * M * N : nullptr;
         for (int c = 0; c < N; c += 8) {
             uint32_t r[8];
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
@@ -260,9 +290,9 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
                     v[j] = __uint_as_float(r[j]) + (bias ? bias[c + j] : 0.f);
                     if (relu) v[j] = fmaxf(v[j], 0.f);
                 }
-                if (Y32) {
+                if (Yp) {
 #pragma unroll
-                    for (int j = 0; j < 8; j++) Y32[(long long)m * N + c + j] = v[j];
+                    for (int j = 0; j < 8; j++) Yp[(long long)m * N + c + j] = v[j];
                 }
                 if (Y16) {
                     __nv_bfloat162 h[4];
@@ -279,6 +309,15 @@ __global__ void __launch_bounds__(128) k_gemm_tc(const __nv_bfloat16* __restrict
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(N) : "memory");
+}
+
+// Y[i] = sum over splits s of P[s][i], in split order
+__global__ void k_sum_splits(long long n, int splits, const float* __restrict__ P, float* __restrict__ Y) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float v = 0.f;
+        for (int s = 0; s < splits; s++) v += P[(long long)s * n + i];
+        Y[i] = v;
+    }
 }
 
 // out[c * ldo + r] = in[r * C + c] for r < R, c < C, and 0 for R <= r < ldo: a BF16 transpose

@@ -3,6 +3,7 @@
 // sequences of its forward pass, backward pass and Adam step (kernels in ud_mlp.cuh).
 // Included by ud_engine.cu after its device-buffer helpers.
 #pragma once
+#include <cudaTypedefs.h>
 #include <random>
 
 struct MlpState {
@@ -76,15 +77,73 @@ struct MlpState {
 
     static constexpr int TC_SMEM = 96 * 1024;   // more than the 48 KB of stages: at most 2 CTAs
                                                 // per SM, so 2 x 256 tensor-memory columns fit
+    DBuf<float> part;                            // split-K partial sums of the weight gradients
+
+    // the driver's tensor-map encoder, looked up once through the runtime
+    static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
+        static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+        if (!fn) {
+            void* f = nullptr;
+            cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+            ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
+            if (q != cudaDriverEntryPointSuccess || !f) throw Fail(UD_ECUDA, "cuTensorMapEncodeTiled is not available");
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        }
+        return fn;
+    }
+    static CUtensorMap encode(const __nv_bfloat16* base, const cuuint64_t dim[3], const cuuint64_t str[2],
+                              const cuuint32_t box[3], const char* what) {
+        CUtensorMap m;
+        const cuuint32_t es[3] = {1, 1, 1};
+        const CUresult r = encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(base), dim, str,
+                                     box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) throw Fail(UD_ECUDA, std::string("cuTensorMapEncodeTiled failed for ") + what);
+        return m;
+    }
+    // X operand: rows x K (K a multiple of 8) BF16 values, row stride ld; K-major 128-row boxes
+    static CUtensorMap map_x(const __nv_bfloat16* base, int rows, int K, int ld) {
+        const cuuint64_t dim[3] = {8, (cuuint64_t)rows, (cuuint64_t)(K / 8)};
+        const cuuint64_t str[2] = {(cuuint64_t)ld * 2, 16};
+        const cuuint32_t box[3] = {8, (cuuint32_t)TC_BM, TC_BK / 8};
+        return encode(base, dim, str, box, "a K-major operand");
+    }
+    // W operand: K rows x N values (row-major); N-major boxes of 32 rows
+    static CUtensorMap map_w(const __nv_bfloat16* base, int K, int N) {
+        const cuuint64_t dim[3] = {8, (cuuint64_t)K, (cuuint64_t)(N / 8)};
+        const cuuint64_t str[2] = {(cuuint64_t)N * 2, 16};
+        const cuuint32_t box[3] = {8, (cuuint32_t)TC_BK, (cuuint32_t)(N / 8)};
+        return encode(base, dim, str, box, "an N-major operand");
+    }
+
+    // one tcgen05 GEMM: Y = act(X W + b); X rows x K with row stride ldx, W K x N; `splits` CTAs
+    // per row tile share the K range (FP32 partials summed in split order into Y32)
+    void tc_run(cudaStream_t s, const __nv_bfloat16* X, int M, int K, int ldx, const __nv_bfloat16* W, int N,
+                const float* bias, int relu, __nv_bfloat16* Y16, float* Y32, int splits) {
+        if (K % 8 || ldx % 8 || (N != 64 && N != 256)) throw Fail(UD_EINVAL, "tensor-core GEMM shape");
+        const int kchunk = ((K + splits - 1) / splits + TC_BK - 1) / TC_BK * TC_BK;
+        const CUtensorMap mx = map_x(X, M, K, ldx), mw = map_w(W, K, N);
+        const dim3 grid((unsigned)((M + TC_BM - 1) / TC_BM), (unsigned)splits);
+        float* y = Y32;
+        if (splits > 1) {
+            part.ensure((size_t)splits * M * N);
+            y = part.p;
+        }
+        if (N == 256)
+            k_gemm_tc<256><<<grid, 128, TC_SMEM, s>>>(mx, mw, bias, M, kchunk, relu, Y16, y, tc_err.p);
+        else
+            k_gemm_tc<64><<<grid, 128, TC_SMEM, s>>>(mx, mw, bias, M, kchunk, relu, Y16, y, tc_err.p);
+        ck(cudaGetLastError(), "k_gemm_tc");
+        if (splits > 1) {
+            const long long nmn = (long long)M * N;
+            k_sum_splits<<<blocks(nmn), 256, 0, s>>>(nmn, splits, part.p, Y32);
+            ck(cudaGetLastError(), "k_sum_splits");
+        }
+    }
 
     void tc_layer(cudaStream_t s, int n, const __nv_bfloat16* x, int K, long long off_w, long long off_b, int N,
                   int relu, __nv_bfloat16* y16, float* y32) {
-        const unsigned grid = (unsigned)((n + TC_BM - 1) / TC_BM);
-        if (N == 256)
-            k_gemm_tc<256><<<grid, 128, TC_SMEM, s>>>(x, p16.p + off_w, p.p + off_b, n, K, relu, y16, y32, tc_err.p);
-        else
-            k_gemm_tc<64><<<grid, 128, TC_SMEM, s>>>(x, p16.p + off_w, p.p + off_b, n, K, relu, y16, y32, tc_err.p);
-        ck(cudaGetLastError(), "k_gemm_tc");
+        tc_run(s, x, n, K, K, p16.p + off_w, N, p.p + off_b, relu, y16, y32, 1);
     }
 
     // errors recorded by the tensor-core GEMM since the last check (call after a sync)
@@ -105,6 +164,7 @@ struct MlpState {
         if (!use_tc || tc_attr) return;
         ck(cudaFuncSetAttribute(k_gemm_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
         ck(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM), "attr");
+        encoder();                                  // the encoder lookup, before any capture
         tc_err.ensure(1);
         ck(cudaMemsetAsync(tc_err.p, 0, sizeof(int), s), "memset");
         tc_attr = true;
@@ -138,20 +198,20 @@ struct MlpState {
         ck(cudaGetLastError(), "k_transpose_bf16");
     }
 
-    // Y[M x N] (FP32) = X[M x K] W[K x N] on the tensor cores, no bias or activation
-    void tc_gemm(cudaStream_t s, const __nv_bfloat16* X, int M, int K, const __nv_bfloat16* W, int N, float* Y) {
-        const unsigned grid = (unsigned)((M + TC_BM - 1) / TC_BM);
-        if (N == 256)
-            k_gemm_tc<256><<<grid, 128, TC_SMEM, s>>>(X, W, nullptr, M, K, 0, nullptr, Y, tc_err.p);
-        else
-            k_gemm_tc<64><<<grid, 128, TC_SMEM, s>>>(X, W, nullptr, M, K, 0, nullptr, Y, tc_err.p);
-        ck(cudaGetLastError(), "k_gemm_tc");
+    // Y[M x N] (FP32) = X[M x K] W[K x N] on the tensor cores, no bias or activation; a long
+    // contraction (the batch, for weight gradients) is split over CTAs to fill the GPU
+    void tc_gemm(cudaStream_t s, const __nv_bfloat16* X, int M, int K, int ldx, const __nv_bfloat16* W, int N,
+                 float* Y) {
+        const int tiles = (M + TC_BM - 1) / TC_BM;
+        int splits = 1;
+        if (K >= 128) splits = std::max(1, std::min(K / 64, 296 / tiles));
+        tc_run(s, X, M, K, ldx, W, N, nullptr, 0, nullptr, Y, splits);
     }
 
     // The backward products on tcgen05.  Weight gradients dW = h_in^T d contract over the batch:
     // h_in is transposed into [K_in x n32] (n32 = n rounded up to 32, zero tail) and d16 holds
-    // n32 rows with a zero tail, so K = n32 meets the kernel's multiple-of-32 rule.  Input
-    // gradients dh = d W^T take W transposed into [N_out x K_in].
+    // n32 rows with a zero tail; the contraction is split over CTAs (tc_gemm).  Input gradients
+    // dh = d W^T take W transposed into [N_out x K_in].
     void backward_tc(cudaStream_t s, int n, const __nv_bfloat16* x) {
         prepare(s);
         const int n32 = pad32(n);
@@ -164,10 +224,10 @@ struct MlpState {
         k_f32_to_bf16<<<blocks(no), 256, 0, s>>>(no, dout.p, d16.p);
         // output layer: dW4 = h3^T d [256 x 64], db4 = colsum(d), dh3 = d W4^T [n x 256]
         transpose(s, h16[2].p, n, mlp::HID, xt16.p, n32);
-        tc_gemm(s, xt16.p, mlp::HID, n32, d16.p, mlp::OUT, g.p + mlp::OFF_W4);
+        tc_gemm(s, xt16.p, mlp::HID, n32, n32, d16.p, mlp::OUT, g.p + mlp::OFF_W4);
         k_colsum<<<1, 64, 0, s>>>(n, mlp::OUT, dout.p, g.p + mlp::OFF_B4);
         transpose(s, w + mlp::OFF_W4, mlp::HID, mlp::OUT, wt16.p, mlp::HID);
-        tc_gemm(s, d16.p, n, mlp::OUT, wt16.p, mlp::HID, dh.p);
+        tc_gemm(s, d16.p, n, mlp::OUT, mlp::OUT, wt16.p, mlp::HID, dh.p);
         const long long off_w[3] = {mlp::OFF_W1, mlp::OFF_W2, mlp::OFF_W3};
         const long long off_b[3] = {mlp::OFF_B1, mlp::OFF_B2, mlp::OFF_B3};
         const long long nh = (long long)n * mlp::HID;
@@ -177,11 +237,11 @@ struct MlpState {
             const __nv_bfloat16* hin = l ? h16[l - 1].p : x;
             const int kin = l ? mlp::HID : mlp::IN;
             transpose(s, hin, n, kin, xt16.p, n32);
-            tc_gemm(s, xt16.p, kin, n32, d16.p, mlp::HID, g.p + off_w[l]);
+            tc_gemm(s, xt16.p, kin, n32, n32, d16.p, mlp::HID, g.p + off_w[l]);
             k_colsum<<<1, 256, 0, s>>>(n, mlp::HID, dpre.p, g.p + off_b[l]);
             if (l > 0) {
                 transpose(s, w + off_w[l], mlp::HID, mlp::HID, wt16.p, mlp::HID);
-                tc_gemm(s, d16.p, n, mlp::HID, wt16.p, mlp::HID, dh.p);
+                tc_gemm(s, d16.p, n, mlp::HID, mlp::HID, wt16.p, mlp::HID, dh.p);
             }
         }
         ck(cudaGetLastError(), "mlp backward");
