@@ -257,7 +257,7 @@ __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
 
 // ---------------------------------------------------------------- topology staging (TMA)
 // A work item's topology blob goes from global to the CTA's shared memory as one bulk
-// asynchronous copy on the tensor-memory-access engine (cp.async.bulk, no multicast),
+// asynchronous copy on the tensor-memory-access engine (cp.async.bulk, into this CTA only),
 // completing on an mbarrier.  Both addresses are 16-byte aligned and the size is a multiple
 // of 16 bytes (blobs are padded to 4 words and start at 4-word offsets); every thread waits
 // on the barrier's phase with a bounded spin.

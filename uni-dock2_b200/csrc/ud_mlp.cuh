@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(GemmArgs g) {
 // Y[M x N] = act(X[M x K] W[K x N] + b) on the 5th-generation tensor cores: one CTA of 128
 // threads per 128-row tile, the FP32 accumulator (128 lanes x N columns) in tensor memory,
 // one thread issuing tcgen05.mma (kind::f16, BF16 operands, M = 128, K = 16 per instruction).
-// Operands arrive 32 K-values at a time by TMA (cp.async.bulk.tensor, no multicast), double
+// Operands arrive 32 K-values at a time by TMA (cp.async.bulk.tensor, each CTA its own), double
 // buffered: while the tensor cores work on one stage the next stage's tiles are loading.  The
 // canonical no-swizzle layouts come straight out of 3-D tensor maps:
 //  * X (K-major): dims (8 k, rows, K/8 chunks), strides (ld*2 B, 16 B), box (8, 128, 4): four
