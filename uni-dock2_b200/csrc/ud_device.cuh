@@ -165,7 +165,17 @@ struct Env {
     const float4* rec;        // x y z type(as float)
     int nrec;
     GridView grid;
+    // the receptor atoms again, sorted into cubic cells of CELL_A (x fastest), for the direct
+    // sums: cell_start[c] .. cell_start[c + 1] are cell c's atoms, in receptor order
+    const float4* rec_cells;
+    const int* cell_start;
+    float cell_o[3];
+    int cdim[3];
 };
+
+// Cell edge of the receptor cell list: a little above the 8 A cutoff, so that two points
+// closer than the cutoff are never two cells apart along an axis, whatever the rounding.
+constexpr float CELL_A = 8.0625f;
 
 __constant__ float c_vdw[NT] = {1.1f, 1.92f, 1.9f, 1.9f, 1.8f, 1.8f, 1.8f, 1.8f, 1.7f, 1.7f, 1.7f,
                                 1.7f, 1.5f, 2.2f, 2.1f, 2.0f, 1.8f, 2.0f, 2.2f, 2.3f, 1.2f};
@@ -193,6 +203,29 @@ __device__ __forceinline__ double cutoff_r2(float ax, float ay, float az, float 
     double dy = __dsub_rn((double)ay, (double)by);
     double dz = __dsub_rn((double)az, (double)bz);
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// f(r) for every receptor atom in the 27 cells around (px, py, pz): a superset of the atoms
+// within the 8 A cutoff (callers keep the cutoff test), cell rows in (z, y) order, each row's
+// x cells contiguous in the sorted array, receptor order within a cell.  Nothing for a
+// non-finite point (such a pose scores +inf).
+template <class F>
+__device__ __forceinline__ void near_receptor(const Env& env, float px, float py, float pz, F&& f) {
+    if (!env.cell_start || !(isfinite(px) && isfinite(py) && isfinite(pz))) return;
+    const int cx = (int)fminf(fmaxf(floorf((px - env.cell_o[0]) * (1.f / CELL_A)), -2.f), (float)env.cdim[0] + 1.f);
+    const int cy = (int)fminf(fmaxf(floorf((py - env.cell_o[1]) * (1.f / CELL_A)), -2.f), (float)env.cdim[1] + 1.f);
+    const int cz = (int)fminf(fmaxf(floorf((pz - env.cell_o[2]) * (1.f / CELL_A)), -2.f), (float)env.cdim[2] + 1.f);
+    const int x0 = max(cx - 1, 0), x1 = min(cx + 1, env.cdim[0] - 1);
+    if (x0 > x1) return;
+#pragma unroll 1
+    for (int q = 0; q < 9; q++) {                         // the 9 (z, y) rows of cells
+        const int y = cy - 1 + q % 3, z = cz - 1 + q / 3;
+        if ((unsigned)y >= (unsigned)env.cdim[1] || (unsigned)z >= (unsigned)env.cdim[2]) continue;
+        const int row = (z * env.cdim[1] + y) * env.cdim[0];
+        const int e = __ldg(env.cell_start + row + x1 + 1);
+#pragma unroll 1
+        for (int j = __ldg(env.cell_start + row + x0); j < e; j++) f(__ldg(env.rec_cells + j));
+    }
 }
 
 // Vina pair energy and dE/dd at surface distance d for a heavy pair with the given
@@ -251,6 +284,7 @@ __device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
     if (t1 == VN_H || t2 == VN_H) return 0.f;
     return vina_ef(d, hyd_pair(t1, t2), hb_pair(t1, t2), f);
 }
+
 
 // ---------------------------------------------------------------- warp helpers
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -674,6 +708,10 @@ __device__ __forceinline__ float intra_atomic(const Topo& T, const float* X, flo
 // escapes every cutoff and box test and gets a finite energy, so Metropolis and the best
 // records could take it; +inf makes the line search, the BFGS revert, Metropolis and the
 // best records all reject it, and changes nothing for finite poses.
+// CELLS: direct sums over the receptor cell list (the refinement and the scoring kernels);
+// otherwise over every kept receptor atom (the search kernels, whose default scoring is the
+// grid, keep the lighter loop and their register budget).
+template <bool CELLS = false>
 __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const float* X, float* F, float vcap,
                                           float slope, float* PB) {
     const int lane = lane_id();
@@ -693,8 +731,7 @@ __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const f
                 if (m >= 0) e_atom = grid_sample(env.grid, m, px, py, pz, fx, fy, fz);
             } else {
                 const float r1 = T.radius(i);
-                for (int j = 0; j < env.nrec; j++) {
-                    const float4 r = __ldg(env.rec + j);
+                auto pair = [&](const float4 r) {
                     const float rv0 = r.x - px, rv1 = r.y - py, rv2 = r.z - pz;
                     const double rr = cutoff_r2(r.x, r.y, r.z, px, py, pz);
                     if (rr < 64.0) {
@@ -705,6 +742,11 @@ __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const f
                         fdr /= rn;
                         fx -= fdr * rv0; fy -= fdr * rv1; fz -= fdr * rv2;
                     }
+                };
+                if constexpr (CELLS) {
+                    near_receptor(env, px, py, pz, pair);
+                } else {
+                    for (int j = 0; j < env.nrec; j++) pair(__ldg(env.rec + j));
                 }
             }
             if (e_atom > 0.f) {
@@ -827,9 +869,10 @@ __device__ __forceinline__ void grad_from_forces(const Topo& T, const Env& env, 
     __syncwarp();
 }
 
+template <bool CELLS = false>
 __device__ UD_EVAL_ATTR float eval_e_grad(const Topo& T, const Env& env, Slot P, float* F, float* G,
                                              float vcap, float slope, float* PB) {
-    float e = eval_e_f(T, env, P.x, F, vcap, slope, PB);
+    float e = eval_e_f<CELLS>(T, env, P.x, F, vcap, slope, PB);
     grad_from_forces(T, env, P, F, G);
     return e;
 }
@@ -977,6 +1020,7 @@ constexpr int LS_TRIALS = 0, LS_INIT = 1, LS_MOVE = 2;
 // BFGS run goes through the same call sites, so that the search loop holds one copy of the
 // evaluation and kinematics code: mode LS_INIT only evaluates Px (energy, gradient into
 // W.g); LS_MOVE sets Pn = Px moved by W.p (a learned MC move) and evaluates Pn likewise.
+template <bool CELLS = false>
 __device__ UD_LS_ATTR float line_search(const Topo& T, const Env& env, Slot Px, Slot Pn, const Work& W,
                                              int dim, float e0, float vcap, float slope, float& alpha_out,
                                              int& n_eval, int mode) {
@@ -990,7 +1034,7 @@ __device__ UD_LS_ATTR float line_search(const Topo& T, const Env& env, Slot Px, 
             apply_update(T, env, Pn, W.p, alpha, W.sc);
         }
         const Slot Q = mode == LS_INIT ? Px : Pn;
-        e_new = eval_e_grad(T, env, Q, W.F, start ? W.g : W.gn, vcap, slope, W.pb);
+        e_new = eval_e_grad<CELLS>(T, env, Q, W.F, start ? W.g : W.gn, vcap, slope, W.pb);
         n_eval++;
         if (start || e_new - e0 < 1e-4f * alpha * pg) break;
         alpha *= 0.5f;
@@ -1001,6 +1045,7 @@ __device__ UD_LS_ATTR float line_search(const Topo& T, const Env& env, Slot Px, 
 
 // BFGS on the pose in slot ix (bfgs.cuh:729-829).  Uses slots ix / ialt / iori; returns
 // the slot index holding the result, whose header[0] is the final energy.
+template <bool CELLS = false>
 __device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots, int stride, int ix, int ialt,
                                     int iori, const Work& W, int max_steps, float vcap, float slope, int& n_eval,
                                     int move_from = -1) {
@@ -1017,7 +1062,7 @@ __device__ __forceinline__ int bfgs(const Topo& T, const Env& env, float* slots,
         if (step >= 0) minus_hv(W.H, W.g, W.p, dim);          // p = -H g
         float alpha;
         const bool mv = step < 0 && move_from >= 0;
-        const float E1 = line_search(T, env, slot_at(slots, stride, mv ? move_from : cur, T.natom),
+        const float E1 = line_search<CELLS>(T, env, slot_at(slots, stride, mv ? move_from : cur, T.natom),
                                      slot_at(slots, stride, mv ? cur : alt, T.natom), W, dim, E, vcap, slope, alpha,
                                      n_eval, step < 0 ? (mv ? LS_MOVE : LS_INIT) : LS_TRIALS);
         if (step < 0) {

@@ -183,7 +183,7 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
     for (int i = lane; i < 3 * T.natom; i += WARP) P.x[i] = x[i];
     if (lane < 3) { P.h[1 + lane] = io.centers[3 * pose + lane]; P.h[4 + lane] = io.rotvecs[3 * pose + lane]; }
     __syncwarp();
-    float e = eval_e_grad(T, env, P, W.F, W.g, vcap, slope, W.pb);
+    float e = eval_e_grad<true>(T, env, P, W.F, W.g, vcap, slope, W.pb);
     if (lane == 0) out_e[pose] = e;
     float* g = out_g + io.goff[pose];
     for (int i = lane; i < 6 + T.ntors; i += WARP) g[i] = W.g[i];
@@ -291,8 +291,7 @@ __global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict_
             float gx, gy, gz;
             if (m >= 0) e_inter += grid_sample(env.grid, m, xi, yi, zi, gx, gy, gz);
         } else {
-            for (int j = 0; j < env.nrec; j++) {
-                float4 r = __ldg(env.rec + j);
+            near_receptor(env, xi, yi, zi, [&](const float4 r) {
                 double rr = cutoff_r2(r.x, r.y, r.z, xi, yi, zi);
                 if (rr < 64.0) {
                     int tj = (int)r.w;
@@ -310,7 +309,7 @@ __global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict_
                             dec[4] += -0.587439f * (d <= -0.7f ? 1.f : (d >= 0.f ? 0.f : -d / 0.7f));
                     }
                 }
-            }
+            });
         }
         if (decomp) {
             float* o = decomp + doff[pose] + 5 * i;
@@ -377,7 +376,7 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
     for (int r = 0; r < rounds; r++) {
         int others[3], k = 0;
         for (int s = 0; s < 4; s++) if (s != cur) others[k++] = s;
-        cur = bfgs(T, env, ws, L.stride, cur, others[0], others[1], W, max_steps, vcap, slope, ne);
+        cur = bfgs<true>(T, env, ws, L.stride, cur, others[0], others[1], W, max_steps, vcap, slope, ne);
         if (ramp) slope = fminf(slope * 100.f, PENALTY_SLOPE);
     }
     copy_words(rec, ws + (size_t)cur * L.stride, nrec);
@@ -1170,6 +1169,10 @@ struct ud_ctx {
     float bias_k = 0.1f;
     // receptor
     std::vector<float4> h_rec;
+    DBuf<float4> d_rec_cells;           // receptor atoms sorted into CELL_A cells (direct sums)
+    DBuf<int> d_cell_start;
+    float cell_o[3] = {0, 0, 0};
+    int cdim[3] = {1, 1, 1};
     DBuf<float4> d_rec;
     // grid
     DBuf<float> d_maps32;
@@ -1243,6 +1246,9 @@ Env make_env(ud_ctx* c, int mode) {
     e.bias_k = c->bias_k;
     e.rec = c->d_rec.p;
     e.nrec = (int)c->h_rec.size();
+    e.rec_cells = c->d_rec_cells.p;
+    e.cell_start = c->d_cell_start.p;
+    for (int a = 0; a < 3; a++) { e.cell_o[a] = c->cell_o[a]; e.cdim[a] = c->cdim[a]; }
     e.grid.f32 = c->d_maps32.p;
     e.grid.f16 = c->d_maps16.p;
     e.grid.use_f16 = (c->grid_prec == UD_GRID_F16 && c->d_maps16.p) ? 1 : 0;
@@ -1356,7 +1362,8 @@ int ud_destroy(ud_ctx* c) {
     if (!c) return UD_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    c->d_rec.release(); c->d_maps32.release(); c->d_maps16.release();
+    c->d_rec.release(); c->d_rec_cells.release(); c->d_cell_start.release();
+    c->d_maps32.release(); c->d_maps16.release();
     c->d_blobs.release(); c->d_ligs.release(); c->d_best.release();
     c->d_order.release(); c->d_items.release(); c->d_counter.release(); c->d_leaders.release(); c->d_counts.release();
     c->d_sel.release(); c->d_selcnt.release(); c->d_nevals.release();
@@ -1393,6 +1400,30 @@ int ud_set_receptor(ud_ctx* c, int n, const float* xyz, const int* types) {
             if (in) c->h_rec.push_back(make_float4(x, y, z, (float)t));
         }
         c->d_rec.upload(c->h_rec.data(), c->h_rec.size(), c->stream);
+        // cell list over the kept region (box +- 8 A): counting sort, stable in receptor order
+        int ncell = 1;
+        for (int a = 0; a < 3; a++) {
+            c->cell_o[a] = c->box_lo[a] - 8.f;
+            c->cdim[a] = (int)std::floor((c->box_hi[a] + 8.f - c->cell_o[a]) * (1.f / CELL_A)) + 1;
+            ncell *= c->cdim[a];
+        }
+        auto cell_of = [&](const float4& r) {
+            const float p[3] = {r.x, r.y, r.z};
+            int q[3];
+            for (int a = 0; a < 3; a++) {
+                const float f = std::floor((p[a] - c->cell_o[a]) * (1.f / CELL_A));
+                q[a] = std::min(std::max((int)f, 0), c->cdim[a] - 1);
+            }
+            return (q[2] * c->cdim[1] + q[1]) * c->cdim[0] + q[0];
+        };
+        std::vector<int> start((size_t)ncell + 1, 0);
+        for (const float4& r : c->h_rec) start[cell_of(r) + 1]++;
+        for (int k = 0; k < ncell; k++) start[k + 1] += start[k];
+        std::vector<float4> sorted(c->h_rec.size());
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (const float4& r : c->h_rec) sorted[fill[cell_of(r)]++] = r;
+        c->d_rec_cells.upload(sorted.data(), sorted.size(), c->stream);
+        c->d_cell_start.upload(start.data(), start.size(), c->stream);
         ck(cudaStreamSynchronize(c->stream), "receptor upload");
         return UD_OK;
     } catch (const Fail& f) {
