@@ -300,8 +300,8 @@ int ud_search_shape(const ud_ctx* ctx, int* out4);
  * -> 64, ReLU, FP32 accumulation on the tensor cores) predicts from a chain's accepted
  * pose a Gaussian (mean, log-variance) over its 6 + T move dimensions [centre shift (3),
  * rotation vector (3), torsion changes (T)]; a sampled move replaces the random draw of
- * mutate_pose_tile (src/cuda/mc.cu:146-256) with probability p_learned.  BFGS, Vina
- * scoring and Metropolis stay as in the plain search.
+ * mutate_pose_tile (src/cuda/mc.cu:146-256); p_learned is the expected share of MC steps
+ * whose move is learned.  BFGS, Vina scoring and Metropolis stay as in the plain search.
  * Features of a pose (672): energies of the first 8 grid maps at each of up to 80 atoms,
  * squashed v/(1+|v|); torsion angles / pi (up to 20); E/(10+|E|); 1; zero padding.
  * Parameters (flat FP32, ud_mlp_param_count of them): W1[672x256], b1, W2[256x256], b2,
@@ -327,9 +327,11 @@ int ud_mlp_loss_grad(ud_ctx* ctx, int n, const float* x, const float* y, const f
 int ud_mlp_train(ud_ctx* ctx, int n, const float* x, const float* y, const float* mask, int epochs, int batch,
                  float lr, uint64_t seed, float* out_epoch_loss);
 /* The MC search of ud_search with learned moves (grid scoring; ligands of at most 80
- * atoms and 20 torsions): every MC step is one launch of all chains, after one batched
- * forward pass of the network over every chain's accepted pose.  p_learned = 0 gives
- * exactly ud_search's chains.  Results as ud_search (ud_get_chain_poses, ud_cluster). */
+ * atoms and 20 torsions): the steps run in blocks of K = floor(1 / p_learned) (at most 8),
+ * each block one launch of all chains after one batched forward pass of the network over
+ * every chain's accepted pose; the learned move replaces the random move of a block's
+ * first step with probability p_learned * K.  p_learned = 0 gives exactly ud_search's
+ * chains.  Results as ud_search (ud_get_chain_poses, ud_cluster). */
 int ud_search_learned(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
                       float p_learned, long long* out_nevals);
 /* Run the plain search (as ud_search_learned with p_learned = 0) and record up to

@@ -115,23 +115,24 @@ def test_best_scores_agree_with_reference_engine(small_system, ref_run):
 
 
 def test_best_score_distribution_vs_reference_engine_screen(tmp_path):
-    """Full searches compared as distributions on the screen workload: 32 config-1 ligands
+    """Full searches compared as distributions on the screen workload: 32 screen ligands
     (12-48 heavy atoms, Poisson(5) torsions) against the 4000-atom synthetic receptor, 128
-    chains x 100 MC steps, opt_steps by the -1 heuristic, 5 refinement rounds, by the
-    reference's own CUDA engine and by this engine (grid-scored search, exact refinement and
-    final scores).  Different random streams, so ligand by ligand the top scores differ either
-    way; as distributions they agree: mean gap (this - reference) within 0.15 kcal/mol, at
-    least 80 % of ligands within 0.3, and this engine better on at least a quarter of them."""
+    chains x 100 MC steps, opt_steps by the -1 heuristic, 5 refinement rounds, 9 poses, by the
+    reference's own CUDA engine (direct pair sums) and by this engine twice: searching on the
+    direct sums as the reference does, and on the grid maps (the shipped default); refinement
+    and final scores are exact pair sums in both.  Different random streams, so ligand by
+    ligand the top scores differ either way.  Direct search against the reference: no
+    systematic gap (mean within 0.1 kcal/mol, this engine better on at least a quarter of the
+    ligands).  Grid search: the interpolation error of the 0.375 A maps shifts the minima the
+    search finds by a few hundredths of a kcal/mol on average, which the exact refinement does
+    not fully remove; mean gap within 0.15 and at least 80 % of ligands within 0.3."""
     if not os.path.exists(EXE):
         pytest.skip("oracle/_ref/udref_dock not built")
-    from ud2b200 import Engine, synth
+    from ud2b200 import Engine, MODE_DIRECT, MODE_GRID, synth
     from ud2b200.batching import heuristic_opt_steps
     from ud2b200.model import Box, parse_ligands, parse_receptor
-    w = synth.WORKLOADS["screen"]
-    rows, center = synth.make_receptor(w["nrec"], w["cube"], 5)
+    rows, ligd, center, w = synth.make_workload("screen", 32, seed=55)
     box = Box.from_center_size(center, [w["box"]] * 3)
-    sizes = synth.ligand_sizes("screen", 32, 55)
-    ligd = {f"s{i:03d}": synth.make_ligand(n, t, 55 * 7919 + i, center) for i, (n, t) in enumerate(sizes)}
     ligs = parse_ligands(ligd)
     opt = heuristic_opt_steps([l.natom for l in ligs], [l.ntors for l in ligs])
     nchain, steps, seed = 128, 100, 3
@@ -146,23 +147,27 @@ def test_best_score_distribution_vs_reference_engine_screen(tmp_path):
     ref = {}
     for fp in glob.glob(str(out / "udref_*.json")):
         ref.update(json.load(open(fp)))
+    theirs = np.array([ref[n][0]["energy"][1] for n in ligd])
     rec = parse_receptor(rows, box)
     eng = Engine(box)
+    gaps = {}
     try:
         eng.set_receptor(rec.xyz, rec.types)
         eng.build_grid(0.375, sorted(set(int(t) for l in ligs for t in l.types if t != 0)))
         eng.add_ligands(ligs)
-        res, _ = eng.dock(seed=seed, nchain=nchain, mc_steps=steps, opt_steps=opt, refine_steps=5, num_pose=9,
-                          rmsd_limit=1.0, energy_range=10.0)
+        for name, mode in (("direct", MODE_DIRECT), ("grid", MODE_GRID)):
+            res, _ = eng.dock(seed=seed, nchain=nchain, mc_steps=steps, opt_steps=opt, refine_steps=5, num_pose=9,
+                              rmsd_limit=1.0, energy_range=10.0, mode=mode)
+            ours = np.array([float(x.terms[0, :3].sum()) for x in res])
+            assert np.all(np.isfinite(ours))
+            gap = ours - theirs
+            gaps[name] = gap
+            print(f"{name} search, 32 screen ligands, 128 x {steps}: gap (this - reference) mean {gap.mean():+.3f}, "
+                  f"median {np.median(gap):+.3f}, within 0.3: {np.mean(gap <= 0.3):.2f}, this better on "
+                  f"{np.mean(gap < -1e-3):.2f}, max {gap.max():+.3f}")
     finally:
         eng.close()
-    ours = np.array([float(x.terms[0, :3].sum()) for x in res])
-    theirs = np.array([ref[n][0]["energy"][1] for n in ligd])
-    gap = ours - theirs
-    print(f"32 screen ligands, 128 x {steps}: gap (this - reference) mean {gap.mean():+.3f}, median "
-          f"{np.median(gap):+.3f}, within 0.3: {np.mean(gap <= 0.3):.2f}, this better on {np.mean(gap < -1e-3):.2f}, "
-          f"max {gap.max():+.3f}")
-    assert np.all(np.isfinite(ours))
-    assert gap.mean() <= 0.15
-    assert np.mean(gap <= 0.3) >= 0.8
-    assert np.mean(gap < -1e-3) >= 0.25
+    assert abs(gaps["direct"].mean()) <= 0.1
+    assert np.mean(gaps["direct"] < -1e-3) >= 0.25
+    assert gaps["grid"].mean() <= 0.15
+    assert np.mean(gaps["grid"] <= 0.3) >= 0.8

@@ -167,6 +167,10 @@ struct PoseIO {
     const long long* goff;   // per pose: offset of gradient in out_g
 };
 
+// CELLS: the direct sums walk the receptor cell list.  Grid scoring never reaches the direct
+// sums, so its launches take the <false> instance and keep the smaller register budget (the cell
+// walk costs k_score 14 registers, which is one resident CTA per SM fewer).
+template <bool CELLS>
 __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int n, PoseIO io, Env env,
                         float vcap, float slope, int ws_max, float* out_e, float* out_g) {
     extern __shared__ __align__(16) float smem[];
@@ -183,7 +187,7 @@ __global__ void k_score(const int* __restrict__ blobs, const LigDev* __restrict_
     for (int i = lane; i < 3 * T.natom; i += WARP) P.x[i] = x[i];
     if (lane < 3) { P.h[1 + lane] = io.centers[3 * pose + lane]; P.h[4 + lane] = io.rotvecs[3 * pose + lane]; }
     __syncwarp();
-    float e = eval_e_grad<true>(T, env, P, W.F, W.g, vcap, slope, W.pb);
+    float e = eval_e_grad<CELLS>(T, env, P, W.F, W.g, vcap, slope, W.pb);
     if (lane == 0) out_e[pose] = e;
     float* g = out_g + io.goff[pose];
     for (int i = lane; i < 6 + T.ntors; i += WARP) g[i] = W.g[i];
@@ -357,6 +361,8 @@ __global__ void k_terms(const int* __restrict__ blobs, const LigDev* __restrict_
 }
 
 // ====================================================================== BFGS batch
+// CELLS as in k_score: refinement on the grid maps takes the <false> instance.
+template <bool CELLS>
 __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__ ligs, int n, const int* item_lig,
                        const long long* item_off, float* recs, Env env, int max_steps, int rounds, float vcap,
                        float slope0, int ramp, int ws_max, int* nevals) {
@@ -376,7 +382,7 @@ __global__ void k_bfgs(const int* __restrict__ blobs, const LigDev* __restrict__
     for (int r = 0; r < rounds; r++) {
         int others[3], k = 0;
         for (int s = 0; s < 4; s++) if (s != cur) others[k++] = s;
-        cur = bfgs<true>(T, env, ws, L.stride, cur, others[0], others[1], W, max_steps, vcap, slope, ne);
+        cur = bfgs<CELLS>(T, env, ws, L.stride, cur, others[0], others[1], W, max_steps, vcap, slope, ne);
         if (ramp) slope = fminf(slope * 100.f, PENALTY_SLOPE);
     }
     copy_words(rec, ws + (size_t)cur * L.stride, nrec);
@@ -621,19 +627,24 @@ __global__ void __launch_bounds__(NT, MINB) k_search(const int* __restrict__ blo
 }
 
 // ====================================================================== learned search
-// The same MC chains as k_search, advanced one step per launch so that every chain's move
-// can come from one batched evaluation of the proposal network: the accepted pose of each
-// chain stays in HBM (`acc`, laid out as the best records) between steps; a step is
-// k_learn_features -> network forward -> k_learn_step -> k_step_advance, captured once as
-// a CUDA graph and replayed mc_steps times.  With p_learned = 0 the chains follow exactly
-// the moves of k_search (same counter-based random stream, same step function).
+// The same MC chains as k_search, advanced a block of K steps per launch so that the
+// proposals of all chains come from one batched evaluation of the proposal network: the
+// accepted pose of each chain stays in HBM (`acc`, laid out as the best records) between
+// launches; a block is k_learn_features -> network forward -> k_learn_step ->
+// k_step_advance, captured once as a CUDA graph and replayed ceil(mc_steps / K) times.
+// The network sees the block's first pose, so a learned move can replace only the block's
+// first random move, with probability q = p_learned * K (p_learned stays the expected share
+// of learned moves).  With p_learned = 0 the chains follow exactly the moves of k_search
+// (same counter-based random stream, same step function).
 struct LearnP {
     uint32_t k0, k1;
     int nchain, opt_steps, randomize;
     int retain;               // poses kept per chain (1..4)
     int ws_max, blob_max;
-    float p_learned;
+    float p_learned;          // q: probability of a learned move at a block's first step
     int nfeat_maps;           // grid maps used as features (<= 8)
+    int block;                // K: MC steps per launch
+    int mc_steps;
 };
 struct MoveSet {              // recorded accepted moves (training data)
     __nv_bfloat16* x;         // [max][672] features of the pose before the move
@@ -701,7 +712,7 @@ __global__ void k_learn_features(const int* __restrict__ blobs, const LigDev* __
     }
 }
 
-__global__ void k_step_advance(int* step_p) { (*step_p)++; }
+__global__ void k_step_advance(int* step_p, int block) { *step_p += block; }
 
 // rotation vector of the rotation taking the old frame of atoms (f0, f1, f2) to the new one
 // (po, pn: the frame's three points, 9 floats each, before and after)
@@ -928,7 +939,8 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
     float* wsbase = smem + sp.blob_max;
     const int warp = threadIdx.x >> 5, lane = lane_id();
     float* ws = wsbase + (size_t)warp * sp.ws_max;
-    const int step = *step_p;
+    const int step0 = *step_p;
+    const int nsteps = min(sp.block, sp.mc_steps - step0);
     unsigned long long my_evals = 0, my_heavy = 0;
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ int s_flag;
@@ -962,7 +974,7 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
             const Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
             Slot SA = slot_at(ws, L.stride, 0, T.natom);
             Retained<RMAX> keep{out, L.stride, sp.retain, 1e9f, 1e9f, 1e9f, 1e9f};
-            if (step == 0) {
+            if (step0 == 0) {
                 load_initial(sblob, SA, T.natom, T.ntors);
                 if (sp.randomize) randomize(T, env, rng, c, sp.nchain, SA, W.g, W.sc);
                 for (int r = 0; r < sp.retain; r++) init_best(out + (long long)r * L.stride, SA, nrec);
@@ -974,15 +986,19 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
                 if (sp.retain > 3) keep.e3 = out[3LL * L.stride];
             }
             __syncwarp();
-            const Proposal prop{(prop_out && step > 0) ? prop_out + g * mlp::OUT : nullptr, sp.p_learned};
-            int ne = 0;
-            bool accepted;
-            const int A = mc_step(T, env, ws, L.stride, 0, W, rng, step, sp.opt_steps, nrec, keep, ne, prop,
-                                  accepted);
-            const Slot SN = slot_at(ws, L.stride, A, T.natom);
-            if (rec_set.count && step > 0) record_move(T, env, accp, SN, accepted, rec_set, g);
+            int ne = 0, A = 0;
+            for (int s = 0; s < nsteps; s++) {
+                const int step = step0 + s;
+                const Proposal prop{(prop_out && step > 0 && s == 0) ? prop_out + g * mlp::OUT : nullptr,
+                                    sp.p_learned};
+                bool accepted;
+                A = mc_step(T, env, ws, L.stride, A, W, rng, step, sp.opt_steps, nrec, keep, ne, prop, accepted);
+                // moves are recorded with blocks of one step (the features are the block's first pose)
+                if (rec_set.count && step > 0)
+                    record_move(T, env, accp, slot_at(ws, L.stride, A, T.natom), accepted, rec_set, g);
+            }
             __syncwarp();
-            copy_words(accp, SN.h, nrec);
+            copy_words(accp, slot_at(ws, L.stride, A, T.natom).h, nrec);
             my_evals += ne;
             my_heavy += (unsigned long long)ne * T.nheavy;
         }
@@ -1306,6 +1322,10 @@ template <typename K>
 void set_smem(K kernel, size_t bytes) {
     ck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "smem attribute");
 }
+
+// The scoring and refinement kernels of a scoring mode: only direct sums walk the cell list.
+auto score_kernel(const Env& env) { return env.mode == UD_MODE_GRID ? k_score<false> : k_score<true>; }
+auto bfgs_kernel(const Env& env) { return env.mode == UD_MODE_GRID ? k_bfgs<false> : k_bfgs<true>; }
 
 }  // namespace
 
@@ -1770,9 +1790,10 @@ int ud_score_batch(ud_ctx* c, int n, const int* pose_lig, const float* coords, c
         dg.ensure(gs);
         int W = pick_warps(c, wsm, 0, 8);
         size_t smem = (size_t)W * wsm * 4;
-        set_smem(k_score, smem);
+        const auto ks = score_kernel(env);
+        set_smem(ks, smem);
         PoseIO io{dl.p, dxo.p, dx.p, dc.p, dr.p, dgo.p};
-        k_score<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm,
+        ks<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm,
                                                               de.p, dg.p);
         ck(cudaGetLastError(), "k_score launch");
         ck(cudaMemcpyAsync(out_e, de.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
@@ -1857,16 +1878,17 @@ int ud_score_batch_timed(ud_ctx* c, int n, const int* pose_lig, const float* coo
         dg.ensure(gs);
         int W = pick_warps(c, wsm, 0, 8);
         size_t smem = (size_t)W * wsm * 4;
-        set_smem(k_score, smem);
+        const auto ks = score_kernel(env);
+        set_smem(ks, smem);
         PoseIO io{dl.p, dxo.p, dx.p, dc.p, dr.p, dgo.p};
         const unsigned grid = (unsigned)((n + W - 1) / W);
         cudaEvent_t e0, e1;
         ck(cudaEventCreate(&e0), "event");
         ck(cudaEventCreate(&e1), "event");
-        k_score<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, de.p, dg.p);
+        ks<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, de.p, dg.p);
         ck(cudaEventRecord(e0, c->stream), "event");
         for (int r = 0; r < repeats; r++)
-            k_score<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, de.p,
+            ks<<<grid, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, de.p,
                                                        dg.p);
         ck(cudaEventRecord(e1, c->stream), "event");
         ck(cudaGetLastError(), "k_score launch");
@@ -1960,8 +1982,9 @@ int ud_bfgs_batch(ud_ctx* c, int n, const int* pose_lig, float* records, int max
         dn.ensure(n);
         int W = pick_warps(c, wsm, 0, 8);
         size_t smem = (size_t)W * wsm * 4;
-        set_smem(k_bfgs, smem);
-        k_bfgs<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, dl.p, dof.p, dr.p, env,
+        const auto kb = bfgs_kernel(env);
+        set_smem(kb, smem);
+        kb<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, dl.p, dof.p, dr.p, env,
                                                              max_steps, rounds, vcap, slope0, ramp, wsm, dn.p);
         ck(cudaGetLastError(), "k_bfgs launch");
         ck(cudaMemcpyAsync(packed.data(), dr.p, tot * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "D2H");
@@ -2216,6 +2239,11 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     sp.p_learned = p_learned;
     sp.retain = c->retain;
     sp.nfeat_maps = std::min(c->nmaps, mlp::NMAP);
+    // K = floor(1 / p_learned), at most 8; 1 while moves are recorded
+    sp.block = record_max > 0 ? 1 : (p_learned > 0.f ? std::max(1, std::min(8, (int)(1.f / p_learned))) : 8);
+    sp.p_learned = std::min(1.f, p_learned * (float)sp.block);
+    sp.mc_steps = mc_steps;
+    const int nblocks = (mc_steps + sp.block - 1) / sp.block;
     auto kern = c->retain > 1
                     ? (P.minb == 4 ? k_learn_step<4, 4> : (P.minb == 2 ? k_learn_step<2, 4, 384> : k_learn_step<3, 4>))
                     : (P.minb == 4 ? k_learn_step<4, 1> : (P.minb == 2 ? k_learn_step<2, 1, 384> : k_learn_step<3, 1>));
@@ -2238,7 +2266,7 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
             k_move_scan<<<1, 1024, 0, c->stream>>>(ms, nch);
             k_move_copy<<<fblocks, 256, 0, c->stream>>>(ms, c->d_x16.p, nch);
         }
-        k_step_advance<<<1, 1, 0, c->stream>>>(c->d_step.p);
+        k_step_advance<<<1, 1, 0, c->stream>>>(c->d_step.p, sp.block);
     } catch (...) {
         cudaStreamEndCapture(c->stream, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -2249,13 +2277,13 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     cudaGraphDestroy(graph);
     ck(ie, "graph instantiate");
     cudaError_t le = cudaSuccess;
-    for (int s = 0; s < mc_steps && le == cudaSuccess; s++) le = cudaGraphLaunch(exec, c->stream);
+    for (int b = 0; b < nblocks && le == cudaSuccess; b++) le = cudaGraphLaunch(exec, c->stream);
     const cudaError_t se = cudaStreamSynchronize(c->stream);
     cudaGraphExecDestroy(exec);
     ck(le, "graph launch");
     ck(se, "learned search");
     if (p_learned > 0.f) c->mlp.check_tc(c->stream);
-    c->counters[2] += (long long)mc_steps * (3 + (feats ? 1 : 0) + (p_learned > 0.f ? 4 : 0) + (record_max > 0 ? 2 : 0));
+    c->counters[2] += (long long)nblocks * (3 + (feats ? 1 : 0) + (p_learned > 0.f ? 4 : 0) + (record_max > 0 ? 2 : 0));
 }
 
 static void read_search_counters(ud_ctx* c) {
@@ -2377,8 +2405,9 @@ static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long l
                 c->d_item_off.upload(io.data(), n, c->stream);
                 int W = pick_warps(c, wsm, 0, 8);
                 size_t smem = (size_t)W * wsm * 4;
-                set_smem(k_bfgs, smem);
-                k_bfgs<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, c->d_item_lig.p,
+                const auto kb = bfgs_kernel(env);
+                set_smem(kb, smem);
+                kb<<<(n + W - 1) / W, 32 * W, smem, c->stream>>>(c->d_blobs.p, c->d_ligs.p, n, c->d_item_lig.p,
                                                                      c->d_item_off.p, c->d_best.p, env, 2,
                                                                      p->refine_steps, VCAP_AUTH, 100.f, 1, wsm,
                                                                      nullptr);
@@ -2879,9 +2908,10 @@ extern "C" int ud_score_batch_noalloc(ud_ctx* c, int n, const int* pose_lig, con
         ck(cudaGetLastError(), "k_pose_offsets launch");
         const int W = pick_warps(c, wsm, 0, 8);
         const size_t smem = (size_t)W * wsm * 4;
-        set_smem(k_score, smem);
+        const auto ks = score_kernel(env);
+        set_smem(ks, smem);
         PoseIO io{d_lig, d_xo, d_x, d_c, d_r, d_go};
-        k_score<<<(n + W - 1) / W, 32 * W, smem, st>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, d_e,
+        ks<<<(n + W - 1) / W, 32 * W, smem, st>>>(c->d_blobs.p, c->d_ligs.p, n, io, env, vcap, slope, wsm, d_e,
                                                        d_g);
         ck(cudaGetLastError(), "k_score launch");
         ck(cudaMemcpyAsync(out_e, d_e, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H");
