@@ -16,12 +16,13 @@ Default (--mode learned):
   end-to-end rate);
 * a proposal network is trained on the GPU from the plain engine's searches of four other
   seeded ligand sets;
-* a step sweep of both engines on batch 0 (--sweep) gives each engine's gate step count, the
-  smallest S with >= 95 % of ligands within 0.3 kcal/mol of the reference;
-* the timed steps dock with the learned engine at its gate step count (`value`, device
-  time; `e2e` through the public API with host buffers); the plain engine at its own gate
-  step count on the same batches is `plain_at_gate`, and `learned_vs_plain_at_gate` their
-  ratio;
+* a step sweep of both engines over all P batches (--sweep) gives each engine's gate step
+  count, the smallest S with >= 95 % of the ligands within 0.3 kcal/mol of the reference;
+* the timed steps dock with the learned engine at --learned-steps (200: its gate count in a
+  sweep over six 148-ligand batches; `value`, device time; `e2e` through the public API
+  with host buffers); the plain engine at its own gate step count on the same batches is
+  `plain_at_gate`, and `learned_vs_plain_at_gate` their ratio; the sweep's `equal_steps`
+  compares both engines at the timed step count;
 * also: the measured L2 and HBM read peaks, a standalone roofline of the scoring kernel on
   ~1e6 resident poses, a 65,536-ligand uneven launch (config 2 scale), the reference's own
   CUDA engine on a small batch when oracle/_ref/udref_dock is built, and the CPU baseline.
@@ -94,8 +95,9 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--grid", default="f32", choices=["f32", "f16"])
     ap.add_argument("--mode", default="learned", choices=["learned", "plain"])
-    ap.add_argument("--learned-steps", type=int, default=400,
-                    help="MC steps of the timed learned-proposal engine (the step sweep's gate count on the screen batch)")
+    ap.add_argument("--learned-steps", type=int, default=200,
+                    help="MC steps of the timed learned-proposal engine (its gate count in a sweep over six "
+                         "148-ligand screen batches)")
     ap.add_argument("--p-learned", type=float, default=0.25, help="share of learned moves")
     ap.add_argument("--train-ligands", type=int, default=37, help="training ligands per seed (4 seeds)")
     ap.add_argument("--train-epochs", type=int, default=6, help="epochs of network training")
@@ -104,7 +106,7 @@ def parse():
     ap.add_argument("--ref-steps", type=int, default=0,
                     help="MC steps of the gate reference (0 = the workload's; smaller only for profiling runs)")
     ap.add_argument("--pool", type=int, default=3, help="fresh ligand batches the timed steps cycle through")
-    ap.add_argument("--sweep", default="50,100,200,400,1000", help="MC steps of the step sweep")
+    ap.add_argument("--sweep", default="100,150,200,250,300,400,1000", help="MC steps of the step sweep")
     ap.add_argument("--no-extras", action="store_true", help="skip the 65,536-ligand and reference-engine blocks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -558,7 +560,7 @@ def run_ours(a):
     import torch
     from ud2b200 import Engine, GRID_F16, GRID_F32, MODE_GRID
     from ud2b200.batching import heuristic_opt_steps
-    from ud2b200.engine import pack_ligands, read_bandwidth
+    from ud2b200.engine import learned_block, pack_ligands, read_bandwidth
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -619,31 +621,42 @@ def run_ours(a):
         extra["learned_training"] = {"train_ligands": sum(len(t) for t in tsets), "ligand_seeds": [101, 102, 103, 104],
                                      "samples": trep.samples, "collect_s": trep.collect_s, "train_s": trep.train_s,
                                      "epoch_loss": trep.epoch_loss, "target": "move to the ligand's best pose"}
-        # step sweep of both engines on pool batch 0; each engine's gate step count is the
-        # smallest S whose share within 0.3 kcal/mol of the reference is >= 95 %
+        # step sweep of both engines over every pool batch; each engine's gate step count is
+        # the smallest S whose share of ligands within 0.3 kcal/mol of the reference, over all
+        # the batches, is >= 95 %; the timed step count is always swept
         sweep = {"plain": [], "learned": []}
         gate_s = {}
+        lt_s = arm_mc_steps(a, w)
+        steps_list = sorted(set([int(v) for v in a.sweep.split(",")] + [lt_s]))
         for eng_name, pl in (("plain", None), ("learned", a.p_learned)):
-            for S in [int(v) for v in a.sweep.split(",")]:
-                res, ms, _, _, _ = dock_timed(eng, pool[0], dict(base_kw, mc_steps=S), flush, p_learned=pl)
-                gap = np.array(top_scores(res)) - refs[0]
+            for S in steps_list:
+                gaps_s, ms_s = [], 0.0
+                for j in range(P):
+                    res, ms, _, _, _ = dock_timed(eng, pool[j], dict(base_kw, mc_steps=S), flush, p_learned=pl)
+                    gaps_s.append(np.array(top_scores(res)) - refs[j])
+                    ms_s += ms
+                gap = np.concatenate(gaps_s)
                 within = float(np.mean(gap <= 0.3))
                 sweep[eng_name].append({"mc_steps": S, "within": within, "mean_gap": float(np.mean(gap)),
-                                        "ligands_per_s": nl / (ms / 1000.0), "ms": ms})
+                                        "ligands_per_s": nl * P / (ms_s / 1000.0), "ms": ms_s / P})
                 if within >= 0.95 and eng_name not in gate_s:
                     gate_s[eng_name] = S
-                elif eng_name in gate_s:
-                    break                      # one more S past the gate, then stop
+                elif eng_name in gate_s and S > lt_s:
+                    break                      # one more S past the gate and the timed count, then stop
         log(f"sweep done: gate MC steps {gate_s}")
         for k in ("plain", "learned"):
-            gate_s.setdefault(k, max(int(v) for v in a.sweep.split(",")))
-        # equal wall time: the plain engine's share within at the learned engine's time per batch
-        lt_s = arm_mc_steps(a, w)
-        lt = next((x["ms"] for x in sweep["learned"] if x["mc_steps"] == lt_s),
-                  next(x["ms"] for x in sweep["learned"] if x["mc_steps"] == gate_s["learned"]))
+            gate_s.setdefault(k, max(steps_list))
+        # equal steps and equal wall time: the plain engine at the learned engine's step count,
+        # and at the most steps it runs in the learned engine's time per batch
+        lt = next(x["ms"] for x in sweep["learned"] if x["mc_steps"] == lt_s)
         eq = [x for x in sweep["plain"] if x["ms"] <= lt * 1.02]
-        extra["sweep"] = {"batch": "pool batch 0", "p_learned": a.p_learned, "plain": sweep["plain"],
-                          "learned": sweep["learned"], "gate_mc_steps": gate_s,
+        same = next((x for x in sweep["plain"] if x["mc_steps"] == lt_s), None)
+        learned_same = next(x for x in sweep["learned"] if x["mc_steps"] == lt_s)
+        extra["sweep"] = {"batches": f"all {P} pool batches ({nl * P} ligands)", "p_learned": a.p_learned,
+                          "plain": sweep["plain"], "learned": sweep["learned"], "gate_mc_steps": gate_s,
+                          "equal_steps": {"mc_steps": lt_s, "plain": same,
+                                          "learned_vs_plain": (learned_same["ligands_per_s"] / same["ligands_per_s"])
+                                          if same else None},
                           "equal_wall_time": {"learned_ms": lt, "plain": eq[-1] if eq else None}}
         run_kw = dict(base_kw, mc_steps=arm_mc_steps(a, w))
         p_learned = a.p_learned
@@ -708,7 +721,7 @@ def run_ours(a):
              "hbm_read_gbs": read_bandwidth(local, 4 << 30, 5)}
     bytes_alg = heavy * 8 * (2 if a.grid == "f16" else 4)
     achieved = bytes_alg / (search_ms / 1000.0) / 1e9 if search_ms > 0 else 0.0
-    launches_per_step = run_kw["mc_steps"] if learned else 1
+    launches_per_step = -(-run_kw["mc_steps"] // learned_block(p_learned)) if learned else 1
     tr = load_traffic("k_learn_step_screen.md" if learned else "k_search_screen.md")
     traffic = tr if (tr is not None and nl == 148 and a.workload == "screen" and a.grid == "f32") else None
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,

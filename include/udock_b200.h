@@ -334,6 +334,10 @@ int ud_mlp_train(ud_ctx* ctx, int n, const float* x, const float* y, const float
  * chains.  Results as ud_search (ud_get_chain_poses, ud_cluster). */
 int ud_search_learned(ud_ctx* ctx, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize,
                       float p_learned, long long* out_nevals);
+/* K, the MC steps per launch of the learned search: floor(1 / p_learned) clamped to 1..8
+ * (8 at p_learned = 0); 1 while moves are recorded (recording != 0) or for p_learned
+ * outside [0, 1].  Needs no device. */
+int ud_learned_block(float p_learned, int recording);
 /* Run the plain search (as ud_search_learned with p_learned = 0) and record up to
  * max_moves accepted moves: the features of the pose before the step, a move (centre
  * shift, rotation vector of a rigid frame of the ligand, wrapped torsion changes) and the

@@ -238,3 +238,16 @@ def test_bench_contract_helpers():
     assert bench.load_traffic("k_learn_step_screen.md") == 24054400.0
     peak, kind = bench.load_peaks()
     assert peak > 1000.0 and kind in ("measured", "fallback")
+
+
+def test_learned_block_sizes(lib):
+    """Steps per launch of the learned search: floor(1 / p) in 1..8, 8 at p = 0, 1 while
+    recording or for an invalid p (no device needed)."""
+    lib.ud_learned_block.argtypes = [C.c_float, C.c_int]
+    lib.ud_learned_block.restype = C.c_int
+    want = {0.0: 8, 0.05: 8, 0.125: 8, 0.2: 5, 0.25: 4, 0.3: 3, 0.5: 2, 0.6: 1, 1.0: 1, -0.1: 1, 1.5: 1}
+    for p, k in want.items():
+        assert lib.ud_learned_block(p, 0) == k, p
+        assert lib.ud_learned_block(p, 1) == 1
+    from ud2b200.engine import learned_block
+    assert learned_block(0.25) == 4 and learned_block(0.25, recording=True) == 1

@@ -2239,8 +2239,7 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     sp.p_learned = p_learned;
     sp.retain = c->retain;
     sp.nfeat_maps = std::min(c->nmaps, mlp::NMAP);
-    // K = floor(1 / p_learned), at most 8; 1 while moves are recorded
-    sp.block = record_max > 0 ? 1 : (p_learned > 0.f ? std::max(1, std::min(8, (int)(1.f / p_learned))) : 8);
+    sp.block = ud_learned_block(p_learned, record_max > 0);
     sp.p_learned = std::min(1.f, p_learned * (float)sp.block);
     sp.mc_steps = mc_steps;
     const int nblocks = (mc_steps + sp.block - 1) / sp.block;
@@ -2485,6 +2484,11 @@ static int dock_impl(ud_ctx* c, const ud_dock_params* p, float p_learned, long l
 }
 
 int ud_dock(ud_ctx* c, const ud_dock_params* p, long long* out_nevals) { return dock_impl(c, p, -1.f, out_nevals); }
+
+int ud_learned_block(float p_learned, int recording) {
+    if (recording || !(p_learned >= 0.f && p_learned <= 1.f)) return 1;
+    return p_learned > 0.f ? std::max(1, std::min(8, (int)(1.f / p_learned))) : 8;
+}
 
 int ud_dock_learned(ud_ctx* c, const ud_dock_params* p, float p_learned, long long* out_nevals) {
     if (!(p_learned >= 0.f && p_learned <= 1.f)) {

@@ -45,6 +45,11 @@ def read_bandwidth(device: int, nbytes: int, repeats: int = 20) -> float:
     return float(out.value)
 
 
+def learned_block(p_learned: float, recording: bool = False) -> int:
+    """MC steps per launch of the learned search for p_learned (ud_learned_block)."""
+    return int(load_library().ud_learned_block(float(p_learned), int(recording)))
+
+
 def load_library() -> C.CDLL:
     """Load the CUDA engine; raises EngineError when it has not been built."""
     global _lib
@@ -101,6 +106,7 @@ def load_library() -> C.CDLL:
         "ud_collect_moves": ([vp, C.c_uint64, i, i, i, i, i, i, C.POINTER(C.c_int)], i),
         "ud_get_moves": ([vp, i, fp, fp, fp], i),
         "ud_dock_learned": ([vp, vp, f, C.POINTER(C.c_longlong)], i),
+        "ud_learned_block": ([f, i], i),
         "ud_mlp_train_moves": ([vp, i, i, f, C.c_uint64, fp], i),
         "ud_read_bandwidth": ([i, C.c_longlong, i, fp], i),
         "ud_score_batch_timed": ([vp, i, ip, fp, fp, fp, i, f, f, i, fp, fp, fp], i),
