@@ -28,7 +28,7 @@ Default (--mode learned):
   CUDA engine on a small batch when oracle/_ref/udref_dock is built, and the CPU baseline.
 --mode plain times the fused 4000-step engine instead.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu|learned-eval]
                     [--mode learned|plain]
 
 N > 1 runs under torchrun, one rank per GPU, each rank docking its own ligands (weak
@@ -84,7 +84,9 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu", "learned-eval"])
+    ap.add_argument("--eval-ligands", type=int, default=4096, help="fresh ligands of the learned-eval run")
+    ap.add_argument("--eval-steps", default="1000", help="MC steps per chain of the learned-eval run (list)")
     ap.add_argument("--ref-ligands", type=int, default=8, help="ligands of the reference-gpu comparison")
     ap.add_argument("--ref-mc-steps", type=int, default=100, help="MC steps of the reference-gpu comparison")
     ap.add_argument("--workload", default="screen")
@@ -422,6 +424,73 @@ def run_reference_gpu(a, emit: bool = True):
                    f"from {steps} to {w['mc_steps']} MC steps"}
     if emit:
         emit_line(out)
+    return out
+
+
+def run_learned_eval(a):
+    """Learned proposal against the plain engine on fresh screen ligands (the learned-proposal
+    benchmark configuration): --eval-ligands fresh ligands (1024 per launch) docked by the
+    plain fused engine and by the learned engine at each of --eval-steps MC steps per chain
+    (equal steps), and by the plain engine at the step count that fills the learned engine's
+    device time on the first batch (equal wall time); the network is trained as in the
+    default run.  Best scores are compared ligand by ligand: mean gap (learned - plain),
+    share within 0.3 kcal/mol, share where the learned engine is better.  Run on demand."""
+    import numpy as np
+    import torch
+    from ud2b200 import Engine, MODE_GRID
+    from ud2b200.batching import heuristic_opt_steps
+    from ud2b200.learned import train_proposal
+    w, box, rec, _ = make_inputs("screen", 1, a.seed, 0)
+    center = (box.lo.astype(np.float64) + box.hi) / 2.0
+    n, per = a.eval_ligands, 1024
+    batches = [ligand_batch("screen", min(per, n - j * per), a.seed * 1000 + 500 + j, 0, center)
+               for j in range((n + per - 1) // per)]
+    tsets = train_sets("screen", a.train_ligands, center)
+    opt = heuristic_opt_steps([l.natom for b in batches for l in b], [l.ntors for b in batches for l in b])
+    mt = sorted(set(int(t) for ls in batches + tsets for l in ls for t in l.types if t != 0))
+    eng = Engine(box)
+    eng.set_receptor(rec.xyz, rec.types)
+    eng.build_grid(0.375, mt)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda:0")
+    params, trep = train_proposal(box, rec, tsets, mt, opt_steps=opt, nchain=w["chains"], mc_steps=150, target=1,
+                                  epochs=a.train_epochs, batch=1024, lr=1e-3, seed=1, device=0,
+                                  max_moves=a.train_moves)
+    eng.mlp_set_params(params)
+    kw = dict(seed=a.seed, nchain=w["chains"], opt_steps=opt, refine_steps=5, num_pose=w["num_pose"],
+              rmsd_limit=w["rmsd"], energy_range=10.0, randomize=True, mode=MODE_GRID)
+    out = {"impl": "learned-eval", "workload": "screen", "ligands": n, "chains": w["chains"], "opt_steps": opt,
+           "p_learned": a.p_learned, "train_samples": trep.samples, "results": []}
+
+    def cmp(x, y):
+        g = x - y
+        return {"mean_gap": float(g.mean()), "within_0.3": float(np.mean(np.abs(g) <= 0.3)),
+                "learned_better": float(np.mean(g < -1e-3)), "plain_better": float(np.mean(g > 1e-3))}
+
+    for S in [int(v) for v in a.eval_steps.split(",")]:
+        top = {"plain": [], "learned": [], "plain_eq": []}
+        ms = {"plain": 0.0, "learned": 0.0, "plain_eq": 0.0}
+        s_eq = None
+        for j, ls in enumerate(batches):
+            for name, steps, pl in (("plain", S, None), ("learned", S, a.p_learned)):
+                res, t, _, _, _ = dock_timed(eng, ls, dict(kw, mc_steps=steps), flush, p_learned=pl)
+                top[name].append(np.array(top_scores(res)))
+                ms[name] += t
+            if s_eq is None:
+                s_eq = int(round(S * ms["learned"] / ms["plain"]))
+            res, t, _, _, _ = dock_timed(eng, ls, dict(kw, mc_steps=s_eq), flush)
+            top["plain_eq"].append(np.array(top_scores(res)))
+            ms["plain_eq"] += t
+            log(f"learned-eval S={S}: batch {j + 1}/{len(batches)}")
+        t = {k: np.concatenate(v) for k, v in top.items()}
+        out["results"].append({
+            "mc_steps": S,
+            "plain": {"ligands_per_s": n / (ms["plain"] / 1000.0), "mean_top": float(t["plain"].mean())},
+            "learned": {"ligands_per_s": n / (ms["learned"] / 1000.0), "mean_top": float(t["learned"].mean())},
+            "equal_steps": cmp(t["learned"], t["plain"]),
+            "equal_wall_time": dict(cmp(t["learned"], t["plain_eq"]), plain_mc_steps=s_eq,
+                                    plain_ligands_per_s=n / (ms["plain_eq"] / 1000.0))})
+    eng.close()
+    emit_line(out)
     return out
 
 
@@ -791,6 +860,8 @@ def main():
         run_reference(a)
     elif a.impl == "reference-gpu":
         run_reference_gpu(a)
+    elif a.impl == "learned-eval":
+        run_learned_eval(a)
     else:
         run_ours(a)
 
