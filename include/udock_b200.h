@@ -275,24 +275,23 @@ int ud_counters(const ud_ctx* ctx, long long* out4);
 int ud_set_retain(ud_ctx* ctx, int retain);
 
 /* Chain packing autotuner for ud_search / ud_dock (on != 0): before a batch of a new
- * shape, times short searches (3 MC steps) with 8, 12 or 4 warps per CTA and keeps the
- * fastest.  Results do not depend on the
+ * shape, times short searches (3 MC steps) with 8, 12 or 4 warps per CTA and 1, 2 or 4
+ * chains per warp per work item and keeps the fastest.  Results do not depend on the
  * packing.  Without it (and without ud_set_packing) the search takes the CTA width that
  * keeps the most warps resident.
  * No reference counterpart (the reference launches one fixed shape, src/cuda/mc.cu:424-440). */
 int ud_set_autotune(ud_ctx* ctx, int on);
 
 /* Fixed chain packing for the searches of this context: warps per CTA (4, 8 or 12; 0 =
- * chosen per batch).  Takes precedence over the autotuner; a width whose CTA does not fit the
- * shared memory falls back to the widest of at most 4 warps that fits (ud_search_shape
- * reports what ran).  chains_per_warp (0..4) is checked and otherwise unused: the warps of a
- * CTA take their ligand's chains one at a time.  Results do not depend on the packing.
+ * chosen per batch) and chains per warp per work item (1..4; 0 = chosen per batch).  Takes
+ * precedence over the autotuner; a width whose CTA does not fit the shared memory falls back
+ * to the widest of at most 4 warps that fits (ud_search_shape reports what ran).  Results do
+ * not depend on the packing.
  * No reference counterpart. */
 int ud_set_packing(ud_ctx* ctx, int warps_per_cta, int chains_per_warp);
 
 /* Launch shape of the last search (fused or learned): out4 = [warps per CTA, CTAs per SM,
- * register class (3, 4: 256-thread bound; 2: 384-thread bound), chains a warp takes at a
- * time (1)].
+ * register class (3, 4: 256-thread bound; 2: 384-thread bound), chains per warp per item].
  * No reference counterpart. */
 int ud_search_shape(const ud_ctx* ctx, int* out4);
 

@@ -193,10 +193,9 @@ def test_autotuned_packing_gives_the_same_chains(gpu_sys):
 
 
 def test_packings_give_the_same_chains(gpu_sys):
-    """Every chain packing (4, 8 or 12 warps per CTA; the warps of a CTA take their ligand's
-    chains one at a time, several CTAs share a ligand) runs the same chains: bit-identical
-    records.  The 12-warp CTAs use the 384-thread instantiation, the others the 256-thread
-    ones."""
+    """Every chain packing (4, 8 or 12 warps per CTA; 1 or 2 chains per warp per work item)
+    runs the same chains: bit-identical records.  The 12-warp CTAs use the 384-thread
+    instantiation, the others the 256-thread ones."""
     eng = gpu_sys["eng"]
     nl = len(gpu_sys["ligs"])
     eng.search(seed=7, nchain=40, mc_steps=8, opt_steps=6, randomize=True)
@@ -207,7 +206,7 @@ def test_packings_give_the_same_chains(gpu_sys):
             eng.set_packing(w, k)
             eng.search(seed=7, nchain=40, mc_steps=8, opt_steps=6, randomize=True)
             sh = eng.search_shape()
-            assert sh["warps_per_cta"] == w and sh["chains_per_warp"] == 1 and sh["ctas_per_sm"] >= 1, sh
+            assert sh["warps_per_cta"] == w and sh["chains_per_warp"] == k and sh["ctas_per_sm"] >= 1, sh
             assert sh["register_class"] == (2 if w == 12 else sh["register_class"])
             for l in range(nl):
                 assert np.array_equal(eng.chain_poses(l), want[l], equal_nan=True), (w, k, l)

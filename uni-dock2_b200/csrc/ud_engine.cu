@@ -548,37 +548,21 @@ __device__ __forceinline__ int mc_step(const Topo& T, const Env& env, float* ws,
     return A;
 }
 
-// Work is claimed per ligand: the slot list repeats the ligands in descending cost a few
-// times; a CTA takes slots from a global counter (work_counter[0]), skips ligands whose
-// chains are all taken, stages the ligand's topology blob, and its warps then take that
-// ligand's chains one by one from the ligand's global counter (work_counter[1 + ligand]),
-// which the other CTAs on the ligand share.  A CTA so waits for its slowest warp only when
-// its ligand runs out of chains, not after every few chains, and CTAs that run out early
-// join the most expensive ligands still running.
+// Work items are (ligand, first chain, chain count) in descending ligand cost; CTAs take
+// items from a global counter, re-stage the topology blob only when the ligand changes,
+// and their warps take the item's chains from a shared counter.  Large ligands are so
+// spread over many CTAs and the launch ends with the cheapest items.
 // NT, MINB: the largest CTA and the CTAs per SM the register budget is sized for (256
 // threads: 4 CTAs = 64 registers, 3 = 80; 384 threads: 2 CTAs = 80 registers); the host
 // picks the width and instantiation that keep the most warps resident (shared memory
 // holds one topology blob per CTA, so wide CTAs pay when the blob is large).
-// One thread: the next slot whose ligand still has chains to take, or -1 when the slots are
-// used up.  A ligand read as open may run out before the CTA's warps reach it; they then
-// take no chain and the CTA claims again.
-__device__ __forceinline__ int claim_ligand(const int4* __restrict__ slots, int nslots, int* work_counter,
-                                            int nchain) {
-    while (true) {
-        const int it = atomicAdd(work_counter, 1);
-        if (it >= nslots) return -1;
-        const int lig = slots[it].x;
-        if (*reinterpret_cast<volatile int*>(work_counter + 1 + lig) < nchain) return lig;
-    }
-}
-
 template <int MINB, int RMAX, int NT = 256>
 __global__ void __launch_bounds__(NT, MINB) k_search(const int* __restrict__ blobs,
                                                 const LigDev* __restrict__ ligs, const int4* __restrict__ items,
                                                 int nitems, Env env, SearchP sp, float* best, int* work_counter,
                                                 unsigned long long* nevals) {
     extern __shared__ __align__(16) float smem[];
-    __shared__ int s_item, s_lig;
+    __shared__ int s_item, s_next, s_lig;
     int* sblob = reinterpret_cast<int*>(smem);
     float* wsbase = smem + sp.blob_max;
     const int warp = threadIdx.x >> 5, lane = lane_id();
@@ -589,25 +573,27 @@ __global__ void __launch_bounds__(NT, MINB) k_search(const int* __restrict__ blo
     uint32_t phase = 0;
     if (threadIdx.x == 0) { s_lig = -1; stage_bar_init(&s_bar); }
     while (true) {
-        if (threadIdx.x == 0) s_item = claim_ligand(items, nitems, work_counter, sp.nchain);
+        if (threadIdx.x == 0) { s_item = atomicAdd(work_counter, 1); s_next = 0; }
         __syncthreads();
-        const int lig = s_item;
-        if (lig < 0) break;
-        const LigDev L = ligs[lig];
-        if (lig != s_lig && !stage_blob(sblob, blobs + L.blob_off, L.stage_words, &s_bar, phase, &s_flag)) {
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 item = items[it];          // (ligand, first chain, count, -)
+        const LigDev L = ligs[item.x];
+        if (item.x != s_lig && !stage_blob(sblob, blobs + L.blob_off, L.stage_words, &s_bar, phase, &s_flag)) {
             if (threadIdx.x == 0 && nevals) atomicAdd(nevals + 2, 1ull);
             break;
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_lig = lig;
+        if (threadIdx.x == 0) s_lig = item.x;
         const Topo T = topo_view(sblob);
         const int nrec = 8 + 3 * T.natom + T.ntors;
         const Work W = work_at(ws, T);
         while (true) {
-            int c = 0;
-            if (lane == 0) c = atomicAdd(work_counter + 1 + lig, 1);
-            c = __shfl_sync(FULL, c, 0);
-            if (c >= sp.nchain) break;
+            int ci = 0;
+            if (lane == 0) ci = atomicAdd(&s_next, 1);
+            ci = __shfl_sync(FULL, ci, 0);
+            if (ci >= item.z) break;
+            const int c = item.y + ci;
             float* out = best + L.best_off + (long long)c * sp.retain * L.stride;
             Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
             int A = 0;
@@ -948,7 +934,7 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
                                                         const __nv_bfloat16* __restrict__ X, MoveSet rec_set,
                                                         int* work_counter, unsigned long long* nevals) {
     extern __shared__ __align__(16) float smem[];
-    __shared__ int s_item, s_lig;
+    __shared__ int s_item, s_next, s_lig;
     int* sblob = reinterpret_cast<int*>(smem);
     float* wsbase = smem + sp.blob_max;
     const int warp = threadIdx.x >> 5, lane = lane_id();
@@ -961,26 +947,28 @@ __global__ void __launch_bounds__(NT, MINB) k_learn_step(const int* __restrict__
     uint32_t phase = 0;
     if (threadIdx.x == 0) { s_lig = -1; stage_bar_init(&s_bar); }
     while (true) {
-        if (threadIdx.x == 0) s_item = claim_ligand(items, nitems, work_counter, sp.nchain);
+        if (threadIdx.x == 0) { s_item = atomicAdd(work_counter, 1); s_next = 0; }
         __syncthreads();
-        const int lig = s_item;
-        if (lig < 0) break;
-        const LigDev L = ligs[lig];
-        if (lig != s_lig && !stage_blob(sblob, blobs + L.blob_off, L.stage_words, &s_bar, phase, &s_flag)) {
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 item = items[it];
+        const LigDev L = ligs[item.x];
+        if (item.x != s_lig && !stage_blob(sblob, blobs + L.blob_off, L.stage_words, &s_bar, phase, &s_flag)) {
             if (threadIdx.x == 0 && nevals) atomicAdd(nevals + 2, 1ull);
             break;
         }
         __syncthreads();
-        if (threadIdx.x == 0) s_lig = lig;
+        if (threadIdx.x == 0) s_lig = item.x;
         const Topo T = topo_view(sblob);
         const int nrec = 8 + 3 * T.natom + T.ntors;
         const Work W = work_at(ws, T);
         while (true) {
-            int c = 0;
-            if (lane == 0) c = atomicAdd(work_counter + 1 + lig, 1);
-            c = __shfl_sync(FULL, c, 0);
-            if (c >= sp.nchain) break;
-            const long long g = (long long)lig * sp.nchain + c;
+            int ci = 0;
+            if (lane == 0) ci = atomicAdd(&s_next, 1);
+            ci = __shfl_sync(FULL, ci, 0);
+            if (ci >= item.z) break;
+            const int c = item.y + ci;
+            const long long g = (long long)item.x * sp.nchain + c;
             float* out = best + L.best_off + (long long)c * sp.retain * L.stride;
             float* accp = acc + L.best_off + (long long)c * L.stride;
             const Rng rng{sp.k0, sp.k1, (uint32_t)c, (uint32_t)L.lig_uid};
@@ -1246,8 +1234,8 @@ struct ud_ctx {
     DBuf<float> d_sy, d_sm;
     int moves_max = 0, moves_n = 0;
     // chain packing autotuner (warps per CTA, chains per warp per work item)
-    int autotune = 0, tune_w = 8;
-    int pack_w = 0;                           // ud_set_packing (0: chosen per batch)
+    int autotune = 0, tune_w = 8, tune_k = 0;
+    int pack_w = 0, pack_k = 0;               // ud_set_packing (0: chosen per batch)
     int shape[4] = {0, 0, 0, 0};              // last search: W, CTAs per SM, minb, k
     int retain = 1;                                   // poses kept per chain
     long long tune_key = -1;
@@ -2022,7 +2010,6 @@ int ud_bfgs_batch(ud_ctx* c, int n, const int* pose_lig, float* records, int max
 // count) in descending ligand cost, uploaded with the work counter cleared.
 struct SearchPlan {
     int W = 0, grid = 0, nitems = 0, wsm = 0, blob_max = 0;
-    int ncounter = 1;      // ints of the work counter: slot cursor, then one chain counter per ligand
     int minb = 3;          // instantiation: 3 or 4 (256-thread bound), 2 (384-thread bound)
     size_t smem = 0;
     long long tot = 0;
@@ -2030,7 +2017,7 @@ struct SearchPlan {
 
 extern "C++" {
 template <typename K>
-static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, K k12, int want_w = 0) {
+static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, K k12, int want_w = 0, int force_k = 0) {
     SearchPlan P;
     const int nlig = (int)c->h_ligs.size();
     std::vector<int> order(nlig);
@@ -2078,24 +2065,26 @@ static SearchPlan plan_search(ud_ctx* c, int nchain, K k3, K k4, K k12, int want
     set_smem(chosen, P.smem);      // the candidates may have set a smaller size on the same kernel
     if (per_sm < 1) per_sm = 1;
     const long long resident = (long long)c->nsm * per_sm;
-    // Slots: the ligands in descending cost, repeated J times, J = 2 + resident CTAs per
-    // ligand, so that every CTA finds a ligand to join while chains are left; a CTA's warps
-    // take the ligand's chains one by one (claim_ligand, k_search).
+    // k chains per warp per item (W*k chains; the warps of a CTA share an item's chains
+    // dynamically): one by default.  Larger items shorten the wait at an item's end relative
+    // to its length but lengthen the launch's tail; on a 148-ligand screen batch (12-warp
+    // CTAs, 400 MC steps) the search took 5.65 s at k = 1, 5.81 s at 2, 5.9-6.1 s at 3 and
+    // 5.8-6.3 s at 4.  The autotuner and ud_set_packing can choose others.
     const long long total_chains = (long long)nlig * nchain;
-    const int J = 2 + (int)((resident + nlig - 1) / std::max(nlig, 1));
+    const int k = force_k > 0 ? force_k : 1;
+    const int item_chains = P.W * k;
     std::vector<int4> items;
-    items.reserve((size_t)J * nlig);
-    for (int pass = 0; pass < J; pass++)
-        for (int l : order) items.push_back(make_int4(l, 0, nchain, pass));
+    for (int l : order)
+        for (int c0 = 0; c0 < nchain; c0 += item_chains)
+            items.push_back(make_int4(l, c0, std::min(item_chains, nchain - c0), 0));
     upload_ligdev(c);
     c->d_items.upload(items.data(), items.size(), c->stream);
     P.nitems = (int)items.size();
-    P.grid = (int)std::min((total_chains + P.W - 1) / P.W, resident);
-    c->shape[0] = P.W; c->shape[1] = per_sm; c->shape[2] = P.minb; c->shape[3] = 1;
-    P.ncounter = 1 + nlig;
-    c->d_counter.ensure((size_t)P.ncounter);
+    P.grid = (int)std::min((long long)P.nitems, resident);
+    c->shape[0] = P.W; c->shape[1] = per_sm; c->shape[2] = P.minb; c->shape[3] = k;
+    c->d_counter.ensure(1);
     c->d_nevals.ensure(3);          // evaluations, heavy-atom evaluations, staging timeouts
-    ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int) * (size_t)P.ncounter, c->stream), "memset");
+    ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
     ck(cudaMemsetAsync(c->d_nevals.p, 0, 3 * sizeof(unsigned long long), c->stream), "memset");
     c->counters[3] = total_chains;
     return P;
@@ -2109,9 +2098,9 @@ static SearchKernel search_kernel(int minb, int rmax) {
     if (rmax > 1) return minb == 4 ? k_search<4, 4> : (minb == 2 ? k_search<2, 4, 384> : k_search<3, 4>);
     return minb == 4 ? k_search<4, 1> : (minb == 2 ? k_search<2, 1, 384> : k_search<3, 1>);
 }
-static SearchPlan plan_fused(ud_ctx* c, int nchain, int want_w = 0) {
+static SearchPlan plan_fused(ud_ctx* c, int nchain, int want_w = 0, int force_k = 0) {
     const int r = c->retain;
-    return plan_search(c, nchain, search_kernel(3, r), search_kernel(4, r), search_kernel(2, r), want_w);
+    return plan_search(c, nchain, search_kernel(3, r), search_kernel(4, r), search_kernel(2, r), want_w, force_k);
 }
 
 static void run_search_plan(ud_ctx* c, const SearchPlan& P, const Env& env, uint64_t seed, int nchain, int mc_steps,
@@ -2135,10 +2124,10 @@ static void run_search_plan(ud_ctx* c, const SearchPlan& P, const Env& env, uint
     }
 }
 
-// Chain packing autotuner: warps per CTA (8, 12 or 4), each timed with CUDA events on a
-// short search of the batch itself (3 MC steps); the fastest is kept for batches of the
-// same shape.  A chain's result does not depend on the packing (its random stream is
-// indexed by chain, ligand and step).
+// Chain packing autotuner: warps per CTA (8, 12 or 4) and chains per warp per work item
+// (1, 2 or 4), each timed with CUDA events on a short search of the batch itself
+// (3 MC steps); the fastest is kept for batches of the same shape.  A chain's result does
+// not depend on the packing (its random stream is indexed by chain, ligand and step).
 static void autotune_search(ud_ctx* c, const Env& env, uint64_t seed, int nchain, int opt_steps, int randomize) {
     const long long key = (long long)c->h_ligs.size() * 1000003LL + (long long)nchain * 131LL + c->max_stage * 7LL +
                           c->retain;
@@ -2147,31 +2136,33 @@ static void autotune_search(ud_ctx* c, const Env& env, uint64_t seed, int nchain
     ck(cudaEventCreate(&e0), "event");
     ck(cudaEventCreate(&e1), "event");
     float best_ms = 1e30f;
-    int best_w = 8;
-    for (int w : {8, 12, 4}) {
-        const SearchPlan P = plan_fused(c, nchain, w);
-        c->d_best.ensure((size_t)P.tot);
-        ck(cudaEventRecord(e0, c->stream), "event");
-        run_search_plan(c, P, env, seed, nchain, 3, opt_steps, randomize);
-        ck(cudaEventRecord(e1, c->stream), "event");
-        ck(cudaEventSynchronize(e1), "autotune");
-        float ms = 0.f;
-        ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
-        if (ms < best_ms) { best_ms = ms; best_w = w; }
-    }
+    int best_w = 8, best_k = 0;
+    for (int w : {8, 12, 4})
+        for (int k : {1, 2, 4}) {
+            const SearchPlan P = plan_fused(c, nchain, w, k);
+            c->d_best.ensure((size_t)P.tot);
+            ck(cudaEventRecord(e0, c->stream), "event");
+            run_search_plan(c, P, env, seed, nchain, 3, opt_steps, randomize);
+            ck(cudaEventRecord(e1, c->stream), "event");
+            ck(cudaEventSynchronize(e1), "autotune");
+            float ms = 0.f;
+            ck(cudaEventElapsedTime(&ms, e0, e1), "event time");
+            if (ms < best_ms) { best_ms = ms; best_w = w; best_k = k; }
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     c->tune_key = key;
     c->tune_w = best_w;
+    c->tune_k = best_k;
 }
 
 static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode) {
     sync_ligs(c);
     Env env = make_env(c, mode);
     c->nchain = nchain * c->retain;                  // records per ligand
-    if (c->autotune && !c->pack_w) autotune_search(c, env, seed, nchain, opt_steps, randomize);
-    const SearchPlan P = c->pack_w      ? plan_fused(c, nchain, c->pack_w)
-                         : c->autotune ? plan_fused(c, nchain, c->tune_w)
+    if (c->autotune && !(c->pack_w || c->pack_k)) autotune_search(c, env, seed, nchain, opt_steps, randomize);
+    const SearchPlan P = (c->pack_w || c->pack_k) ? plan_fused(c, nchain, c->pack_w, c->pack_k)
+                         : c->autotune         ? plan_fused(c, nchain, c->tune_w, c->tune_k)
                                                : plan_fused(c, nchain);
     c->best_floats = P.tot;
     c->d_best.ensure((size_t)P.tot);
@@ -2195,11 +2186,16 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     for (const LigHost& h : c->h_ligs)
         if (h.natom > mlp::NATOM || h.ntors > mlp::TMAX)
             throw Fail(UD_EINVAL, "the proposal network covers ligands of at most 80 atoms and 20 torsions");
+    // two chains per warp per work item unless fixed: a launch runs one MC step of every
+    // chain, whose lengths vary far more than those of whole chains, and sharing an item's
+    // chains among its warps evens them out (148-ligand screen batch, 200 steps, p_learned
+    // 0.25: 2.46 s at k = 2, 2.58 s at 1, 2.56 s at 3, 2.73 s at 4)
+    const int lk = c->pack_k ? c->pack_k : 2;
     const SearchPlan P = c->retain > 1
                              ? plan_search(c, nchain, k_learn_step<3, 4>, k_learn_step<4, 4>, k_learn_step<2, 4, 384>,
-                                           c->pack_w)
+                                           c->pack_w, lk)
                              : plan_search(c, nchain, k_learn_step<3, 1>, k_learn_step<4, 1>, k_learn_step<2, 1, 384>,
-                                           c->pack_w);
+                                           c->pack_w, lk);
     c->best_floats = P.tot;
     c->d_best.ensure((size_t)P.tot);
     c->d_acc.ensure((size_t)P.tot);
@@ -2256,7 +2252,7 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     ck(cudaStreamSynchronize(c->stream), "learned search setup");
     ck(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
     try {
-        ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int) * (size_t)P.ncounter, c->stream), "memset");
+        ck(cudaMemsetAsync(c->d_counter.p, 0, sizeof(int), c->stream), "memset");
         if (feats)
             k_learn_features<<<fblocks, 256, 0, c->stream>>>(c->d_blobs.p, c->d_ligs.p, nlig, nchain, env, c->d_acc.p,
                                                              c->d_step.p, sp.nfeat_maps, c->d_x16.p);
@@ -2594,7 +2590,8 @@ int ud_set_packing(ud_ctx* c, int warps_per_cta, int chains_per_warp) {
         g_err = "packing: warps per CTA 0, 4, 8 or 12; chains per warp 0..4";
         return UD_EINVAL;
     }
-    c->pack_w = warps_per_cta;               // chains per warp: accepted, no longer used
+    c->pack_w = warps_per_cta;
+    c->pack_k = chains_per_warp;
     return UD_OK;
 }
 

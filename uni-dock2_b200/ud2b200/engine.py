@@ -355,8 +355,8 @@ class Engine:
         self._check(self.L.ud_set_autotune(self.h, int(bool(on))))
 
     def set_packing(self, warps_per_cta: int = 0, chains_per_warp: int = 0):
-        """Fix the chain packing (4, 8 or 12 warps per CTA; 0 = chosen per batch);
-        chains_per_warp (0..4) is checked and otherwise unused.  Results do not depend on it."""
+        """Fix the chain packing (4, 8 or 12 warps per CTA; 1..4 chains per warp per item;
+        0 = chosen per batch).  Results do not depend on it."""
         self._check(self.L.ud_set_packing(self.h, int(warps_per_cta), int(chains_per_warp)))
 
     def search_shape(self) -> dict:
