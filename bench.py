@@ -221,29 +221,34 @@ def cpu_port_rate(w, box, rec, ligs, mc_steps, opt_steps, seconds: float, mode: 
     cores = os.cpu_count() or 1
     sample = ligs[:cores]
     oligs = [orc.ligand(l) for l in sample]
-    done_steps = 0
+    done_steps, nchains = 0, 0
     t0 = time.perf_counter()
     steps = 1
+    rnd = 0
+    # rounds of one chain per core (at most mc_steps steps each, fresh chains every round)
+    # until `seconds` have passed
     while True:
-        def run(k):
+        def run(k, rnd=rnd, steps=steps):
             l = sample[k % len(sample)]
             pose = O.initial_pose(l)
-            orc.mc_chain(oligs[k % len(sample)], env, pose, seed=11, lig_uid=k, chain=k, nchain=w["chains"],
-                         mc_steps=steps, opt_steps=opt_steps, randomize=True)
+            ch = rnd * cores + k
+            orc.mc_chain(oligs[k % len(sample)], env, pose, seed=11, lig_uid=k, chain=ch % w["chains"],
+                         nchain=w["chains"], mc_steps=steps, opt_steps=opt_steps, randomize=True)
             return steps
         ts = time.perf_counter()
         with ThreadPoolExecutor(max_workers=cores) as ex:
             done_steps += sum(ex.map(run, range(cores)))
+        nchains += cores
+        rnd += 1
         el = time.perf_counter() - t0
-        if el >= seconds or steps >= mc_steps:
+        if el >= seconds:
             break
-        left = seconds - el
         per = (time.perf_counter() - ts) / steps
-        steps = max(1, min(mc_steps, int(left / max(per, 1e-6))))
+        steps = max(1, min(mc_steps, int((seconds - el) / max(per, 1e-6))))
     el = time.perf_counter() - t0
     rate = done_steps / el
-    return rate, cores, f"{done_steps} MC steps of {cores} chains (one per core) on {len(sample)} screen ligands, " \
-                        f"{mode} scoring, in {el:.1f} s"
+    return rate, cores, f"{done_steps} MC steps of {nchains} chains ({cores} at a time, one per core, at most " \
+                        f"{mc_steps} steps each) on {len(sample)} screen ligands, {mode} scoring, in {el:.1f} s"
 
 
 def reference_scoring_rate(rec, box, ligs, seconds: float = 8.0):
