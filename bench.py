@@ -143,7 +143,7 @@ def load_peaks():
 
 def load_traffic(summary: str = "k_search_screen.md"):
     """DRAM bytes (read + write) of one launch of the dominant kernel at the default batch
-    (k_search, or k_learn_step: one MC step of every chain), from the committed ncu
+    (k_search, or k_learn_step: one block of MC steps of every chain), from the committed ncu
     summary of that launch."""
     p = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(p):

@@ -10,8 +10,8 @@
 //   k_cluster      CTA per ligand: energy ranking + greedy RMSD leaders (src/cuda/cluster.cu)
 //   k_filter       CTA per ligand: energy_range / num_pose filter (src/task/DockTask.cpp:188-220)
 //   k_gather       output records of the selected poses
-//   k_learn_step   one MC step of every chain per launch (the learned-proposal search; the
-//                  step function is k_search's), with k_learn_features (network input per
+//   k_learn_step   a block of K MC steps of every chain per launch (the learned-proposal
+//                  search; the step function is k_search's), with k_learn_features (network input per
 //                  chain), k_step_advance, and k_lig_best / k_label_moves (move recording)
 //   k_pose_offsets prefix sums for ud_score_batch_noalloc
 // Network kernels (tcgen05 forward GEMM, mma.sync GEMM, loss, backward, Adam): ud_mlp.cuh.
@@ -2170,7 +2170,7 @@ static void launch_search(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, in
 }
 
 // The learned-proposal search (and, with record, the collection of accepted moves): one
-// CUDA graph per MC step, replayed mc_steps times.
+// CUDA graph per block of K MC steps, replayed ceil(mc_steps / K) times.
 static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, int opt_steps, int randomize, int mode,
                            float p_learned, int record_max, int target = 0) {
     if (mc_steps < 1) throw Fail(UD_EINVAL, "the learned search needs mc_steps >= 1");
@@ -2186,10 +2186,10 @@ static void launch_learned(ud_ctx* c, uint64_t seed, int nchain, int mc_steps, i
     for (const LigHost& h : c->h_ligs)
         if (h.natom > mlp::NATOM || h.ntors > mlp::TMAX)
             throw Fail(UD_EINVAL, "the proposal network covers ligands of at most 80 atoms and 20 torsions");
-    // two chains per warp per work item unless fixed: a launch runs one MC step of every
-    // chain, whose lengths vary far more than those of whole chains, and sharing an item's
-    // chains among its warps evens them out (148-ligand screen batch, 200 steps, p_learned
-    // 0.25: 2.46 s at k = 2, 2.58 s at 1, 2.56 s at 3, 2.73 s at 4)
+    // two chains per warp per work item unless fixed: a launch runs a block of a few MC steps
+    // of every chain, whose lengths vary far more than those of whole chains, and sharing an
+    // item's chains among its warps evens them out (148-ligand screen batch, 200 steps,
+    // p_learned 0.25, blocks of 4 steps: 1683 ms at k = 2, 1718 at 1, 1808 at 4)
     const int lk = c->pack_k ? c->pack_k : 2;
     const SearchPlan P = c->retain > 1
                              ? plan_search(c, nchain, k_learn_step<3, 4>, k_learn_step<4, 4>, k_learn_step<2, 4, 384>,
