@@ -1,7 +1,7 @@
 """GPU parity of every intra-pair evaluation path against the FP64 oracle.
 
-Ligand sizes straddle the path boundary: the register round robin (<= 32 atoms) and the
-pair list with the per-warp pair buffer (> 32), up to 80 atoms.  Energies and generalised
+Ligand sizes from 12 to 80 atoms, through the pair list with the per-warp pair buffer
+(every ligand whose list fits it).  Energies and generalised
 gradients within 1e-4 relative, grid and direct scoring, curl caps 10 and off.
 """
 import numpy as np

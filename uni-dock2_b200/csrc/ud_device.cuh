@@ -53,8 +53,6 @@ enum BlobHdr {
     H_MAPIDX,      // natom ints: grid map slot of each atom (-1: none), set at upload
     H_NPREC,       // number of heavy scored pairs (a count, not an offset)
     H_PREC,        // 2 words per pair: i | j<<12 | hydrophobic<<24 | hbond<<25, and R_i + R_j (float)
-    H_AFLAGS,      // natom ints: heavy | hydrophobic<<1 | acceptor<<2 | donor<<3
-    H_PMASK,       // natom <= 32: one word per atom, bit b set if the heavy pair (a, b) is scored
     H_GOFF,        // natom+1 ints: per-atom lists of (pair index, partner) for the gather
     H_GADJ,        // entries: pair index | partner << 16
     H_TOTAL,
@@ -62,7 +60,6 @@ enum BlobHdr {
     H_FRAME0,      // 3 words: non-collinear atoms no torsion moves (a rigid frame), or -1
     H_WORDS = 36
 };
-constexpr int AF_HEAVY = 1, AF_HYD = 2, AF_ACC = 4, AF_DON = 8;
 // The search is bound by instruction fetch: its loop body is large and the warps of an SM
 // run different parts of it.  Every loop with a run-time trip count therefore carries
 // `#pragma unroll 1`; the compiler's default unrolling of those loops made the library's
@@ -78,13 +75,6 @@ constexpr int AF_HEAVY = 1, AF_HYD = 2, AF_ACC = 4, AF_DON = 8;
 #ifndef UD_LS_ATTR
 #define UD_LS_ATTR __forceinline__
 #endif
-#ifndef RR32_MAX_ATOMS
-#define RR32_MAX_ATOMS 32      // ligands up to this size use the register round robin (<= 32)
-#endif
-// intra-pair path of a ligand of n atoms: 0 register round robin (one atom per lane),
-// 2 the pair list (pair buffer or atomics).  A round robin with two atoms per lane was
-// measured 1.5x slower on the search than the pair buffer (shuffle-bound, spills).
-__host__ __device__ __forceinline__ int intra_path(int n) { return n <= RR32_MAX_ATOMS ? 0 : 2; }
 constexpr int PREC_HYD = 1 << 24, PREC_HB = 1 << 25;
 constexpr int PAIR_ZERO = 1 << 16, PAIR_HYD = 1 << 17, PAIR_HB = 1 << 18;
 
@@ -93,7 +83,7 @@ struct Topo {
     const int* b;
     int natom, ntors, nheavy, nbias;
     int o_types, o_axis, o_roff, o_ranges, o_rot_off, o_rot, o_pair_off, o_pairs, o_bias_off, o_bias, o_heavy,
-        o_radii, o_rhoff, o_rheavy, o_mapidx, nprec, o_prec, o_aflags, o_pmask, o_goff, o_gadj;
+        o_radii, o_rhoff, o_rheavy, o_mapidx, nprec, o_prec, o_goff, o_gadj;
     __device__ __forceinline__ int type(int i) const { return b[o_types + i]; }
     __device__ __forceinline__ int axis(int k) const { return b[o_axis + k]; }
     __device__ __forceinline__ int range_off(int k) const { return b[o_roff + k]; }
@@ -110,8 +100,6 @@ struct Topo {
     __device__ __forceinline__ int rheavy(int q) const { return b[o_rheavy + q]; }
     __device__ __forceinline__ int map_index(int i) const { return b[o_mapidx + i]; }
     __device__ __forceinline__ int2 prec(int p) const { return *reinterpret_cast<const int2*>(b + o_prec + 2 * p); }
-    __device__ __forceinline__ int aflags(int i) const { return b[o_aflags + i]; }
-    __device__ __forceinline__ unsigned pmask(int i) const { return (unsigned)b[o_pmask + i]; }
     __device__ __forceinline__ int goff(int i) const { return b[o_goff + i]; }
     __device__ __forceinline__ int gadj(int k) const { return b[o_gadj + k]; }
 };
@@ -140,8 +128,6 @@ __device__ __forceinline__ Topo topo_view(const int* b) {
     t.o_mapidx = b[H_MAPIDX];
     t.nprec = b[H_NPREC];
     t.o_prec = b[H_PREC];
-    t.o_aflags = b[H_AFLAGS];
-    t.o_pmask = b[H_PMASK];
     t.o_goff = b[H_GOFF];
     t.o_gadj = b[H_GADJ];
     return t;
@@ -273,10 +259,6 @@ __device__ __forceinline__ float pair_scalar(float dx, float dy, float dz, float
     }
     s_out = fdr;
     return ep;
-}
-__device__ __forceinline__ bool flags_hyd(int fa, int fb) { return (fa & fb & AF_HYD) != 0; }
-__device__ __forceinline__ bool flags_hb(int fa, int fb) {
-    return ((fa & AF_ACC) && (fb & AF_DON)) || ((fa & AF_DON) && (fb & AF_ACC));
 }
 
 __device__ __forceinline__ float eval_ef(float d, int t1, int t2, float& f) {
@@ -602,53 +584,14 @@ __device__ __forceinline__ float grid_sample(const GridView& g, int map, float x
 // bfgs.cuh:305-352).  Both visits give the same energy and opposite forces, so each
 // heavy pair is evaluated once here.  The functions add the intra forces to F (which
 // holds the inter forces of the lane's own atoms) and return the lane's share of the
-// intra energy.  The kernel is issue bound, so each variant keeps the number of
-// evaluated pair slots close to the number of pairs.
+// intra energy.  The kernel is issue bound, so both variants evaluate exactly the listed
+// pairs, spread evenly over the lanes.  (A round robin in registers for ligands of up to 32
+// atoms, one atom per lane and partners fetched by shuffle, visited every atom pair slot and
+// was measured 11 % slower on the plain search of a screen batch, 17 % on the learned one.)
 
-// natom = n <= 32: a round robin in registers.  Lane a < n owns atom a; in round
-// t = 1..n/2 it pairs with atom (a + t) mod n, fetched by shuffle (in the last round of an
-// even n only a < n/2 computes), keeps the force on its own atom and hands the reaction
-// back by shuffle.  Every pair is visited once in n/2 rounds; no shared memory, no
-// atomics, fixed summation order.
-__device__ __forceinline__ float intra_rr32(const Topo& T, const float* X, float* F, float vcap) {
-    const int a = lane_id();
-    const int n = T.natom;
-    const bool va = a < n;
-    float xa = 0.f, ya = 0.f, za = 0.f, Ra = 0.f;
-    int fa = 0;
-    unsigned ma = 0u;
-    if (va) {
-        xa = X[3 * a]; ya = X[3 * a + 1]; za = X[3 * a + 2];
-        Ra = T.radius(a); fa = T.aflags(a); ma = T.pmask(a);
-    }
-    const int rounds = n >> 1;
-    const int half = (n & 1) ? WARP : rounds;          // last round of an even n: a < n/2 only
-    float fx = 0.f, fy = 0.f, fz = 0.f, e = 0.f;
-#pragma unroll 1
-    for (int t = 1; t <= rounds; t++) {
-        int b = a + t, src = a - t;                    // partner, and the lane that paired with a
-        if (b >= n) b -= n;
-        if (src < 0) src += n;
-        if (!va) { b = a; src = a; }
-        const float xb = __shfl_sync(FULL, xa, b), yb = __shfl_sync(FULL, ya, b), zb = __shfl_sync(FULL, za, b);
-        const float Rb = __shfl_sync(FULL, Ra, b);
-        const int fb = __shfl_sync(FULL, fa, b);
-        const float dx = xb - xa, dy = yb - ya, dz = zb - za;
-        float sc = 0.f;
-        if (((ma >> b) & 1u) && (t < rounds || a < half))
-            e += pair_scalar(dx, dy, dz, Ra + Rb, flags_hyd(fa, fb), flags_hb(fa, fb), vcap, sc);
-        const float px = -sc * dx, py = -sc * dy, pz = -sc * dz;       // force on a
-        fx += px - __shfl_sync(FULL, px, src);
-        fy += py - __shfl_sync(FULL, py, src);
-        fz += pz - __shfl_sync(FULL, pz, src);
-    }
-    if (va) { F[3 * a] += fx; F[3 * a + 1] += fy; F[3 * a + 2] += fz; }
-    return e;
-}
-
-// more than 32 atoms: pass 1 evaluates every pair once, pairs spread evenly over the
-// lanes, and stores the force scalar of each pair in the warp's pair buffer PB; pass 2
-// gathers F_a += s_p (x_a - x_b) over the atom's pairs in pair-index order
+// Pass 1 evaluates every pair once and stores the force scalar of each pair in the warp's
+// pair buffer PB; pass 2 gathers F_a += s_p (x_a - x_b) over the atom's pairs in pair-index
+// order
 __device__ __forceinline__ float intra_buffered(const Topo& T, const float* X, float* F, float vcap, float* PB) {
     const int lane = lane_id();
     float e = 0.f;
@@ -702,7 +645,7 @@ __device__ __forceinline__ float intra_atomic(const Topo& T, const float* X, flo
 
 // ---------------------------------------------------------------- energy + force
 // Fills F (3N, dE/dx per atom) and returns the warp-summed energy (bfgs.cuh:221-394).
-// PB: the warp's pair buffer for ligands above 32 atoms (null: atomic accumulation).
+// PB: the warp's pair buffer (null when the pair list does not fit it: atomic accumulation).
 // A pose with a non-finite coordinate scores +inf.  In the reference such a pose (left by
 // a rotation increment whose norm overflows, quaternion.h:90-107 then gives sin(inf))
 // escapes every cutoff and box test and gets a finite energy, so Metropolis and the best
@@ -768,9 +711,7 @@ __device__ __forceinline__ float eval_e_f(const Topo& T, const Env& env, const f
         F[3 * i] = fx; F[3 * i + 1] = fy; F[3 * i + 2] = fz;
     }
     __syncwarp();
-    const int path = intra_path(T.natom);
-    if (path == 0) energy += intra_rr32(T, X, F, vcap);
-    else if (PB) energy += intra_buffered(T, X, F, vcap, PB);
+    if (PB) energy += intra_buffered(T, X, F, vcap, PB);
     else energy += intra_atomic(T, X, F, vcap);
     // bias (bfgs.cuh:356-388; vina.h:353-400)
     if (env.bias_type != 0 && T.nbias > 0) {
@@ -990,7 +931,7 @@ struct Work {        // per-warp scratch in shared memory
     float* mhy;      // D
     float* sc;       // 2T torsion sine/cosine scratch
     double* H;       // D(D+1)/2, packed upper triangle: H[i + j(j+1)/2], i <= j
-    float* pb;       // pair buffer for ligands above 32 atoms, or null
+    float* pb;       // pair buffer (one float per scored pair), or null
 };
 
 __device__ __forceinline__ float gdot(const float* a, const float* b, int n) {

@@ -46,12 +46,12 @@ __host__ __device__ inline int rec_floats(int n, int t) { return r4(8 + 3 * n + 
 #define PB_MAX_FLOATS 4096
 #endif
 constexpr int PB_MAX = PB_MAX_FLOATS;
-__host__ __device__ inline int pb_floats(int n, int npair) {
-    return (intra_path(n) == 2 && npair <= PB_MAX) ? r4(npair) : 0;
+__host__ __device__ inline int pb_floats(int npair) {
+    return npair <= PB_MAX ? r4(npair) : 0;
 }
 __host__ __device__ inline int ws_floats(int n, int t, int npair) {
     int d = 6 + t;
-    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(2 * t) + r4(d * (d + 1)) + pb_floats(n, npair);
+    return 4 * rec_floats(n, t) + r4(3 * n) + 5 * r4(d) + r4(2 * t) + r4(d * (d + 1)) + pb_floats(npair);
 }
 
 struct LigDev {
@@ -76,7 +76,7 @@ __device__ __forceinline__ Work work_at(float* ws, const Topo& T) {
     W.mhy = W.y + r4(d);
     W.sc = W.mhy + r4(d);
     W.H = reinterpret_cast<double*>(W.sc + r4(2 * ntors));
-    W.pb = pb_floats(natom, T.nprec) ? reinterpret_cast<float*>(W.H) + r4(d * (d + 1)) : nullptr;
+    W.pb = pb_floats(T.nprec) ? reinterpret_cast<float*>(W.H) + r4(d * (d + 1)) : nullptr;
     return W;
 }
 
@@ -1609,7 +1609,7 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
             for (int i = 0; i < n; i++) blob[o + i] = -1;
             {   // heavy scored pairs, once each (i < j), for the intra kernels, in round-robin
                 // order (pair (a, a+t mod n) for t = 1..n/2) so that 32 consecutive pairs touch
-                // each atom about twice
+                // each atom about twice (fewer shared-memory bank conflicts in pass 1)
                 std::vector<char> scored((size_t)n * n, 0);
                 for (int i = 0; i < n; i++)
                     for (int k = pair_off[a0 + i] - p0; k < pair_off[a0 + i + 1] - p0; k++) {
@@ -1638,25 +1638,8 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 const int np2 = (int)rec.size() / 2;
                 if (np2 > 0xFFFF) throw Fail(UD_EINVAL, "too many intra pairs (max 65535)");
                 blob[H_NPREC] = np2;
-                // sections the search reads come first: what the register round robin needs
-                // (ligands of at most 32 atoms), then the pair list and gather lists of larger
-                // ligands, then the adjacency only the final scoring reads (not staged)
-                o = put(H_AFLAGS, n);
-                for (int i = 0; i < n; i++) {
-                    const int t = types[a0 + i];
-                    const unsigned b = 1u << t;
-                    blob[o + i] = (t != VN_H ? AF_HEAVY : 0) | ((b & HYD_MASK) ? AF_HYD : 0) |
-                                  ((b & ACC_MASK) ? AF_ACC : 0) | ((b & DON_MASK) ? AF_DON : 0);
-                }
-                const bool rr = intra_path(n) == 0;      // partner masks for the round robin
-                o = put(H_PMASK, rr ? n : 0);
-                if (rr)
-                    for (int p = 0; p < np2; p++) {
-                        const int i = rec[2 * p] & 0xFFF, j = (rec[2 * p] >> 12) & 0xFFF;
-                        blob[o + i] |= (int)(1u << j);
-                        blob[o + j] |= (int)(1u << i);
-                    }
-                const int stage_small = (int)blob.size();
+                // sections the search reads come first: the pair list and gather lists, then
+                // the adjacency only the final scoring reads (not staged)
                 o = put(H_PREC, (int)rec.size());
                 for (size_t q = 0; q < rec.size(); q++) blob[o + q] = rec[q];
                 // gather lists: for each atom, (pair index, partner) in pair-index order
@@ -1673,7 +1656,7 @@ int ud_add_ligands(ud_ctx* c, int nlig, const int* atom_off, const float* xyz, c
                 o = put(H_GADJ, acc);
                 for (int i = 0, k = 0; i < n; i++)
                     for (int v : g[i]) blob[o + k++] = v;
-                blob[H_STAGE] = rr ? stage_small : (int)blob.size();
+                blob[H_STAGE] = (int)blob.size();
             }
             o = put(H_PAIR_OFF, n + 1);
             for (int i = 0; i <= n; i++) blob[o + i] = pair_off[a0 + i] - p0;
