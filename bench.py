@@ -111,7 +111,10 @@ def parse():
     ap.add_argument("--sweep", default="100,150,200,250,300,400,1000", help="MC steps of the step sweep")
     ap.add_argument("--no-extras", action="store_true", help="skip the 65,536-ligand and reference-engine blocks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0,
+                    help="length of the CPU baseline sample of the default run")
+    ap.add_argument("--ref-sample-s", type=float, default=0.0,
+                    help="seconds per step of the reference arm's sample (0: from --steps and --warmup)")
     return ap.parse_args()
 
 
@@ -307,7 +310,7 @@ def run_reference(a):
     mc = arm_mc_steps(a, w)
     opt = heuristic_opt_steps([l.natom for l in batch0], [l.ntors for l in batch0])
     P = max(1, min(a.steps, a.pool))
-    per_step = max(2.0, min(30.0, 120.0 / max(1, a.steps + a.warmup)))
+    per_step = a.ref_sample_s or max(2.0, min(30.0, 120.0 / max(1, a.steps + a.warmup)))
     rates, secs = [], []
     for st in range(a.warmup + a.steps):
         t0 = time.perf_counter()
@@ -846,12 +849,25 @@ def run_ours(a):
         block("reference_gpu", lambda: run_reference_gpu(a, emit=False))
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         def cpu():
+            # the reference arm in a fresh interpreter (no CUDA context, no torch worker
+            # threads competing for the host cores), one step of --cpu-seconds on this
+            # arm's workload
             m = run_kw["mc_steps"]
-            rate, cores, sample = cpu_port_rate(w, box, rec, pool[0], m, opt, a.cpu_seconds)
-            return {"value": rate / (w["chains"] * m), "unit": UNIT, "cores": cores, "kind": "port",
-                    "sample": sample + f"; ligands/s at {m} MC steps per chain (this arm's)"}
+            cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", "1", "--warmup", "0",
+                   "--workload", a.workload, "--ligands", str(a.ligands), "--seed", str(a.seed),
+                   "--mc-steps", str(m), "--ref-sample-s", str(a.cpu_seconds)]
+            env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, env=env)
+            line = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+            if r.returncode != 0 or not line:
+                raise RuntimeError(f"reference arm subprocess rc={r.returncode}: {r.stderr[-300:]}")
+            ref = json.loads(line[-1])
+            cb = dict(ref["cpu_baseline"])
+            cb["sample"] += f"; ligands/s at {m} MC steps per chain (this arm's); a separate process"
+            if ref.get("reference_cpu_scoring"):
+                out["reference_cpu_scoring"] = ref["reference_cpu_scoring"]
+            return cb
         block("cpu_baseline", cpu)
-        block("reference_cpu_scoring", lambda: reference_scoring_rate(rec, box, pool[0]))
     if rank == 0:
         emit_line(out)
     if dist:
