@@ -251,3 +251,26 @@ def test_learned_block_sizes(lib):
         assert lib.ud_learned_block(p, 1) == 1
     from ud2b200.engine import learned_block
     assert learned_block(0.25) == 4 and learned_block(0.25, recording=True) == 1
+
+
+def test_reference_arm_line_contract():
+    """bench.py --impl reference prints one JSON line with the arm's contract keys (a tiny
+    sample: 4 ligands, 2 MC steps, 1 s)."""
+    import subprocess
+    import sys
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--ligands", "4", "--mc-steps", "2", "--ref-sample-s", "1"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench_metric() and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+    assert d["config"]["mc_steps"] == 2 and d["higher_is_better"] is True
+
+
+def bench_metric():
+    with open(os.path.join(ROOT, "BASELINE.json")) as f:
+        return json.load(f)["metric"]
