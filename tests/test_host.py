@@ -235,7 +235,7 @@ def test_bench_contract_helpers():
     with open(os.path.join(ROOT, "BASELINE.json")) as f:
         assert bench.METRIC == json.load(f)["metric"]
     assert bench.load_traffic("k_search_screen.md") == 12984320.0
-    assert bench.load_traffic("k_learn_step_screen.md") == 27304192.0
+    assert bench.load_traffic("k_learn_step_screen.md") == 27495936.0
     peak, kind = bench.load_peaks()
     assert peak > 1000.0 and kind in ("measured", "fallback")
 
