@@ -274,3 +274,22 @@ def test_reference_arm_line_contract():
 def bench_metric():
     with open(os.path.join(ROOT, "BASELINE.json")) as f:
         return json.load(f)["metric"]
+
+
+def test_size_groups_batches_and_opt_steps_rule():
+    """Size groups at their limits (screening.h:19-30: a ligand goes to the first group whose
+    atom and torsion limits it meets), batches of at most 1000 in input order, and the
+    opt_steps = -1 rule from the first batch (screening.cpp:206-208)."""
+    from ud2b200.batching import batches, heuristic_opt_steps, size_groups
+    na = [40, 41, 40, 80, 81, 160, 161, 10]
+    nt = [8, 8, 9, 16, 1, 32, 0, 33]
+    g = size_groups(na, nt)
+    assert g == [[0], [1, 2, 3], [4], [5], [6, 7]]
+    big = [20] * 2500 + [60] * 10
+    b = batches(big, [2] * len(big))
+    assert [len(x) for x in b] == [1000, 1000, 500, 10]
+    assert b[0][0] == 0 and b[2][-1] == 2499 and b[3][0] == 2500
+    assert heuristic_opt_steps(big, [2] * len(big)) == (25 + 20) // 3
+    assert heuristic_opt_steps([], []) == 0
+    # the first batch is the first non-empty group's: medium ligands only
+    assert heuristic_opt_steps([70, 50], [10, 9]) == (25 + 70) // 3
